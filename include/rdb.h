@@ -1,0 +1,184 @@
+/*
+ * rdb.h -- C ABI of the B200 Riemersma engines (librdb_b200.so).
+ *
+ * Plain pointers, sizes and POD structs only; no C++ or CUDA types cross this
+ * boundary (streams travel as void*).  Every entry point returns 0 on success
+ * or an RDB_E_* code; rdb_last_error() then gives a human-readable message
+ * for the calling thread.  The reference's engine API (include/rd_riemersma.h
+ * of rdither) reports errors as a std::string that is empty on success; the
+ * C++ drop-in layer (rd_dropin.cpp) maps these codes back to that form.
+ *
+ * Each declaration names the reference interface it stands in for.
+ */
+#ifndef RDB_H_
+#define RDB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RDB_OK 0
+#define RDB_E_INVALID 1     /* bad argument */
+#define RDB_E_CUDA 2        /* CUDA runtime error, or no usable device */
+#define RDB_E_NOMEM 3       /* device allocation failed or budget exceeded */
+#define RDB_E_UNSUPPORTED 4 /* refused by the engine's stated limits */
+#define RDB_E_DEVICE 5      /* a kernel reported an error status */
+#define RDB_E_TIMEOUT 6     /* a bounded wait expired */
+
+/* Pixel layouts. */
+#define RDB_RGB8 3     /* 3 bytes per pixel */
+#define RDB_RGBA8 4    /* 4 bytes per pixel */
+#define RDB_RGBAF32 16 /* 4 floats per pixel, ImageMagick Q16 range (RgbaF) */
+
+/* Engines. */
+#define RDB_ENGINE_SEQ 0    /* sequential-exact walk (RiemersmaWalkCpu / RiemersmaWalkCuda) */
+#define RDB_ENGINE_BLOCKS 1 /* block-parallel walk (RiemersmaBlocksCpu / RiemersmaBlocksCuda) */
+#define RDB_ENGINE_JACOBI 2 /* order-free approximation (RiemersmaApproxCuda) */
+
+/* Message for the calling thread's last failing call ("" if none). */
+const char* rdb_last_error(void);
+
+/* ---- device ---------------------------------------------------------------
+ * Replaces CudaAvailable() (include/rd_riemersma.h:284). */
+int rdb_device_count(int* count);
+/* Device name as "<name> (sm_XY)", the form RiemersmaWalkCuda reports. */
+int rdb_device_name(int device, char* buf, size_t len);
+/* Replaces CudaAllocPinned / CudaFreePinned (include/rd_riemersma.h:480-481). */
+void* rdb_alloc_pinned(size_t bytes);
+void rdb_free_pinned(void* p);
+
+/* ---- palette building -----------------------------------------------------
+ * Replaces rd::ColorTree::Build (include/rd_octree.h:62-63): ImageMagick's
+ * octree classification, reduction to at most `max_colors` and colormap, on
+ * the host.  `row_stride` is in bytes (0 = packed). */
+typedef struct rdb_octree rdb_octree;
+int rdb_octree_build(const void* pixels, int layout, size_t width, size_t height,
+                     size_t row_stride, int max_colors, int associate_alpha, int grayscale,
+                     rdb_octree** out);
+int rdb_octree_color_count(const rdb_octree* t);
+int rdb_octree_node_count(const rdb_octree* t);
+int rdb_octree_depth(const rdb_octree* t);
+/* count x 4 doubles (r, g, b, a) */
+void rdb_octree_colormap(const rdb_octree* t, double* out);
+/* node_count x 16 child ids, parent, colour number, unique-pixel count */
+void rdb_octree_nodes(const rdb_octree* t, int32_t* child, int32_t* parent,
+                      uint32_t* color_number, uint64_t* number_unique);
+void rdb_octree_free(rdb_octree* t);
+/* 1 when every pixel has r == g == b (the reference's greyscale rule,
+ * src/rd_cli.cpp:2452-2456). */
+int rdb_is_grayscale(const void* pixels, int layout, size_t width, size_t height,
+                     size_t row_stride);
+
+/* ---- context -------------------------------------------------------------
+ * Device state kept across calls: resident palettes, visit-order tables per
+ * geometry, memo slabs and scratch.  The reference keeps comparable state in
+ * its blocks engine's DeviceState slots (src/rd_blocks_cuda.cu:855-1002).
+ * A context is used by one host thread at a time. */
+typedef struct rdb_context rdb_context;
+/* memory_budget: bytes of device memory the context may hold (0 = 90 % of free). */
+int rdb_context_create(int device, size_t memory_budget, rdb_context** out);
+void rdb_context_destroy(rdb_context* ctx);
+/* Device bytes currently held by the context. */
+size_t rdb_context_bytes(const rdb_context* ctx);
+
+/* A palette and its colour tree, in the reference's own terms
+ * (rd::Palette, include/rd_riemersma.h:63-67; rd::QNode, include/rd_octree.h:43-52). */
+typedef struct rdb_palette_desc {
+  int count;                      /* palette entries, 1..256 */
+  int associate_alpha;
+  const double* colors;           /* count x 4 (palette.entries) */
+  const double* search_colors;    /* count x 4 (tree colormap); NULL = colors */
+  int node_count;
+  int root;
+  const int32_t* child;           /* node_count x 16, -1 = none */
+  const int32_t* parent;          /* node_count, may be NULL */
+  const uint32_t* color_number;   /* node_count */
+  const uint64_t* number_unique;  /* node_count */
+} rdb_palette_desc;
+
+int rdb_palette_create(rdb_context* ctx, const rdb_palette_desc* desc, int* palette_id);
+/* The device plan blob for a palette, built on the host (no device needed):
+ * header, palette tables, live child table, per-node search runs and the
+ * post-order slot map (layout in stipple_b200/csrc/rdb_plan.h).  Writes at
+ * most `cap` bytes and the full size to *size. */
+int rdb_plan_build(const rdb_palette_desc* desc, void* out, size_t cap, size_t* size);
+int rdb_palette_from_octree(rdb_context* ctx, const rdb_octree* t, int* palette_id);
+int rdb_palette_destroy(rdb_context* ctx, int palette_id);
+
+/* ---- dithering -----------------------------------------------------------
+ * One image.  Device pointers. */
+typedef struct rdb_job {
+  const void* pixels;   /* device, row-major, `layout` */
+  size_t row_stride;    /* bytes between rows (0 = packed) */
+  int width;
+  int height;
+  int layout;
+  int palette_id;
+  uint8_t* indices;     /* device, width*height bytes: palette index per pixel */
+  float* rgba_out;      /* optional device RgbaF result (width*height*4 floats); may equal
+                           `pixels` for RDB_RGBAF32 (in place, as the reference works) */
+} rdb_job;
+
+typedef struct rdb_options {
+  double diffusion;     /* dither:diffusion-amount, default 1.0 (DitherParams::diffusion) */
+  int use_cache;        /* sequential engine: ImageMagick's memo table, default 1 */
+  int block;            /* blocks engine: positions per block, >= 16, default 512 */
+  int jacobi_iters;     /* default 20 (ApproxOptions::iterations) */
+  int jacobi_taps;      /* default 96 (ApproxOptions::taps), 1..4096 */
+  int jacobi_fp64;      /* default 0 (ApproxOptions::fp64) */
+  int cache_bits;       /* sequential engine: log2 shared-memory memo cache entries, 0 = auto */
+  int reserved[8];
+} rdb_options;
+
+void rdb_options_default(rdb_options* o);
+
+/* Dithers `n_jobs` images with one engine on `stream` (cudaStream_t, NULL =
+ * the context's stream).  The sequential engine runs every job as its own
+ * exact walk inside one persistent launch (a warp per image, longest first);
+ * with n_jobs == 1 it is the plain one-image-per-launch form.  The blocks
+ * engine requires one palette and one layout across the jobs.  Asynchronous:
+ * the call returns after enqueueing; rdb_synchronize() waits and reports any
+ * kernel status.
+ *
+ * Replaces RiemersmaWalkCuda (include/rd_riemersma.h:214-217),
+ * RiemersmaBlocksCuda (:450-464) and RiemersmaApproxCuda (:303-307) at the
+ * device-buffer level. */
+int rdb_dither(rdb_context* ctx, int engine, const rdb_job* jobs, int n_jobs,
+               const rdb_options* opts, void* stream);
+int rdb_synchronize(rdb_context* ctx, void* stream);
+
+/* Host-buffer form: copies `pixels` (host) to the device, dithers, and copies
+ * the index map (and RgbaF result when rgba_out != NULL) back.  Pinned
+ * buffers make the copies asynchronous DMA.  Synchronous. */
+typedef struct rdb_host_job {
+  const void* pixels;
+  size_t row_stride;
+  int width;
+  int height;
+  int layout;
+  int palette_id;
+  uint8_t* indices;     /* host, width*height */
+  float* rgba_out;      /* optional host RgbaF result */
+} rdb_host_job;
+
+int rdb_dither_host(rdb_context* ctx, int engine, const rdb_host_job* jobs, int n_jobs,
+                    const rdb_options* opts);
+
+/* Error weights 16^(-i/15) by ImageMagick's recurrence (rd_types.h:169-176)
+ * and the Jacobi inverse filter (src/rd_approx_cuda.cu:73-88, exposed by the
+ * reference as ApproxInverseFilter). */
+void rdb_error_weights(double out[16]);
+int rdb_inverse_filter(int taps, double diffusion, double* out /* taps+1 */);
+
+/* The block-mode gap: pixel index of the one cell the block list never
+ * visits, or -1 when it lies outside the image (src/rd_riemersma_cpu.cpp:439-455). */
+int64_t rdb_block_gap(int width, int height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RDB_H_ */

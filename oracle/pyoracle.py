@@ -1,0 +1,308 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings for the CPU checkers.
+
+``Oracle`` wraps liboracle.so (the C restatement in oracle.c).  ``RefLib``
+wraps oracle/_ref/librdref.so (the reference's own CPU sources compiled
+unmodified, see oracle/Makefile) and is present only where that library was
+built.  Only tests, the smoke entry point and bench.py's CPU-baseline leg use
+this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "librdref.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+
+def build_oracle() -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")], check=True)
+
+
+class OrcNode(C.Structure):
+    _fields_ = [
+        ("child", C.c_int32 * 16),
+        ("parent", C.c_int32),
+        ("total_color", C.c_double * 4),
+        ("quantize_error", C.c_double),
+        ("number_unique", C.c_uint64),
+        ("color_number", C.c_uint32),
+        ("id", C.c_uint32),
+        ("level", C.c_uint32),
+    ]
+
+
+class OrcTree(C.Structure):
+    _fields_ = [
+        ("nodes", C.POINTER(OrcNode)),
+        ("node_count", C.c_size_t),
+        ("node_cap", C.c_size_t),
+        ("colormap", C.POINTER(C.c_double)),
+        ("color_count", C.c_int),
+        ("maximum_colors", C.c_int),
+        ("depth", C.c_int),
+        ("node_live_count", C.c_size_t),
+        ("pruning_threshold", C.c_double),
+        ("next_threshold", C.c_double),
+        ("associate_alpha", C.c_int),
+        ("root", C.c_int32),
+    ]
+
+
+class Tree:
+    """Result of a palette build: the colormap and the node array."""
+
+    def __init__(self, palette, child, parent, color_number, number_unique, depth, assoc):
+        self.palette = palette  # (count, 4) float64
+        self.child = child  # (nodes, 16) int32
+        self.parent = parent  # (nodes,) int32
+        self.color_number = color_number  # (nodes,) uint32
+        self.number_unique = number_unique  # (nodes,) uint64
+        self.depth = depth
+        self.assoc = assoc
+
+    @property
+    def count(self) -> int:
+        return int(self.palette.shape[0])
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        lib = C.CDLL(path)
+        self.lib = lib
+        lib.orc_tree_build.argtypes = [C.POINTER(OrcTree), _f32p, C.c_size_t, C.c_size_t,
+                                       C.c_int, C.c_int, C.c_int]
+        lib.orc_tree_free.argtypes = [C.POINTER(OrcTree)]
+        lib.orc_walk_seq.argtypes = [C.POINTER(OrcTree), _f64p, C.c_int, C.c_int, C.c_double,
+                                     C.c_int, C.c_size_t, C.c_size_t, _f32p, _u8p]
+        lib.orc_walk_blocks.argtypes = [C.POINTER(OrcTree), _f64p, C.c_int, C.c_int, C.c_double,
+                                        C.c_int, C.c_size_t, C.c_size_t, _f32p, _u8p]
+        lib.orc_walk_blocks.restype = C.c_int
+        lib.orc_seq_order.argtypes = [C.c_size_t, C.c_size_t, _i32p]
+        lib.orc_seq_order.restype = C.c_size_t
+        lib.orc_block_order.argtypes = [C.c_size_t, C.c_size_t, _i32p, _i32p]
+        lib.orc_block_order.restype = C.c_size_t
+        lib.orc_hilbert_point.argtypes = [C.c_int64, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.orc_curve_level.argtypes = [C.c_size_t, C.c_size_t]
+        lib.orc_curve_level.restype = C.c_int
+        lib.orc_scale_quantum_to_char.argtypes = [C.c_float]
+        lib.orc_scale_quantum_to_char.restype = C.c_ubyte
+        lib.orc_build_error_weights.argtypes = [_f64p]
+        lib.orc_inverse_filter.argtypes = [C.c_int, C.c_double, _f64p]
+        lib.orc_tree_lookup.argtypes = [C.POINTER(OrcTree), C.c_double, C.c_double, C.c_double,
+                                        C.c_double]
+        lib.orc_tree_lookup.restype = C.c_int
+
+    # -- palette -------------------------------------------------------------
+    def build_tree_raw(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool):
+        h, w = rgbaf.shape[:2]
+        t = OrcTree()
+        px = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1)
+        self.lib.orc_tree_build(C.byref(t), px, w, h, int(max_colors), int(assoc), int(gray))
+        return t
+
+    def build_tree(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool) -> Tree:
+        t = self.build_tree_raw(rgbaf, max_colors, assoc, gray)
+        try:
+            return self._export(t)
+        finally:
+            self.lib.orc_tree_free(C.byref(t))
+
+    def _export(self, t: OrcTree) -> Tree:
+        n = t.node_count
+        count = t.color_count
+        cm = np.ctypeslib.as_array(t.colormap, shape=(count * 4,)).copy().reshape(count, 4) \
+            if count else np.zeros((0, 4))
+        child = np.empty((n, 16), np.int32)
+        parent = np.empty(n, np.int32)
+        cn = np.empty(n, np.uint32)
+        nu = np.empty(n, np.uint64)
+        arr = (OrcNode * n).from_address(C.addressof(t.nodes.contents))
+        for i in range(n):
+            child[i] = arr[i].child[:]
+            parent[i] = arr[i].parent
+            cn[i] = arr[i].color_number
+            nu[i] = arr[i].number_unique
+        return Tree(cm, child, parent, cn, nu, t.depth, bool(t.associate_alpha))
+
+    # -- walks ---------------------------------------------------------------
+    def walk_seq(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
+                 diffusion: float = 1.0, use_cache: bool = True):
+        """Builds the palette, then the sequential walk.  Returns (idx, out, palette)."""
+        h, w = rgbaf.shape[:2]
+        t = self.build_tree_raw(rgbaf, max_colors, assoc, gray)
+        try:
+            count = t.color_count
+            pal = np.ctypeslib.as_array(t.colormap, shape=(max(count, 1) * 4,)).copy()
+            out = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1).copy()
+            idx = np.zeros(w * h, np.uint8)
+            self.lib.orc_walk_seq(C.byref(t), pal, count, int(assoc), float(diffusion),
+                                  int(use_cache), w, h, out, idx)
+            return idx.reshape(h, w), out.reshape(h, w, 4), pal.reshape(-1, 4)[:count]
+        finally:
+            self.lib.orc_tree_free(C.byref(t))
+
+    def walk_blocks(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
+                    block: int, diffusion: float = 1.0):
+        h, w = rgbaf.shape[:2]
+        t = self.build_tree_raw(rgbaf, max_colors, assoc, gray)
+        try:
+            count = t.color_count
+            pal = np.ctypeslib.as_array(t.colormap, shape=(max(count, 1) * 4,)).copy()
+            out = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1).copy()
+            idx = np.zeros(w * h, np.uint8)
+            rc = self.lib.orc_walk_blocks(C.byref(t), pal, count, int(assoc), float(diffusion),
+                                          int(block), w, h, out, idx)
+            if rc != 0:
+                raise ValueError("blocks walk refused")
+            return idx.reshape(h, w), out.reshape(h, w, 4), pal.reshape(-1, 4)[:count]
+        finally:
+            self.lib.orc_tree_free(C.byref(t))
+
+    # -- curve ----------------------------------------------------------------
+    def seq_order(self, w: int, h: int) -> np.ndarray:
+        out = np.empty(max(w * h, 1), np.int32)
+        n = self.lib.orc_seq_order(w, h, out)
+        return out[:n]
+
+    def block_order(self, w: int, h: int):
+        out = np.empty(w * h + 1, np.int32)
+        owner = np.empty(max(w * h, 1), np.int32)
+        n = self.lib.orc_block_order(w, h, out, owner)
+        return out[:n], owner[: w * h]
+
+    def error_weights(self) -> np.ndarray:
+        w = np.zeros(16, np.float64)
+        self.lib.orc_build_error_weights(w)
+        return w
+
+    def inverse_filter(self, taps: int, diffusion: float = 1.0) -> np.ndarray:
+        g = np.zeros(taps + 1, np.float64)
+        self.lib.orc_inverse_filter(taps, diffusion, g)
+        return g
+
+
+class RefLib:
+    """The reference's own CPU code (oracle/_ref).  Raises if not built."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        lib = C.CDLL(path)
+        self.lib = lib
+        lib.ref_tree_build.argtypes = [_f32p, C.c_size_t, C.c_size_t, C.c_int, C.c_int, C.c_int]
+        lib.ref_tree_build.restype = C.c_void_p
+        lib.ref_tree_free.argtypes = [C.c_void_p]
+        lib.ref_tree_color_count.argtypes = [C.c_void_p]
+        lib.ref_tree_depth.argtypes = [C.c_void_p]
+        lib.ref_tree_node_count.argtypes = [C.c_void_p]
+        lib.ref_tree_node_count.restype = C.c_size_t
+        lib.ref_tree_colormap.argtypes = [C.c_void_p, _f64p]
+        lib.ref_tree_nodes.argtypes = [C.c_void_p, _i32p, _i32p, _u32p, _u64p, _u32p]
+        lib.ref_walk_seq.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_size_t, C.c_size_t, _f32p]
+        lib.ref_walk_blocks.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_size_t, C.c_size_t,
+                                        _f32p, C.c_int, C.c_char_p, C.c_size_t]
+        lib.ref_walk_blocks.restype = C.c_int
+        lib.ref_hilbert_point.argtypes = [C.c_int64, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.ref_curve_level.argtypes = [C.c_size_t, C.c_size_t]
+        lib.ref_block_curve.argtypes = [C.c_size_t, C.c_size_t, _i32p, _i32p]
+        lib.ref_block_curve.restype = C.c_size_t
+        lib.ref_curve_sequence.argtypes = [C.c_int, _i32p]
+        lib.ref_curve_sequence.restype = C.c_size_t
+        lib.ref_curve_mismatches.argtypes = [C.c_int]
+        lib.ref_curve_mismatches.restype = C.c_size_t
+        lib.ref_error_weights.argtypes = [_f64p]
+        lib.ref_scale_char.argtypes = [C.c_float]
+        lib.ref_scale_char.restype = C.c_uint
+
+    def build_tree(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool) -> Tree:
+        h, w = rgbaf.shape[:2]
+        px = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(px, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            return self._export(t, assoc)
+        finally:
+            self.lib.ref_tree_free(t)
+
+    def _export(self, t, assoc) -> Tree:
+        count = self.lib.ref_tree_color_count(t)
+        cm = np.zeros(max(count, 1) * 4, np.float64)
+        self.lib.ref_tree_colormap(t, cm)
+        n = self.lib.ref_tree_node_count(t)
+        child = np.zeros(n * 16, np.int32)
+        parent = np.zeros(n, np.int32)
+        cn = np.zeros(n, np.uint32)
+        nu = np.zeros(n, np.uint64)
+        lv = np.zeros(n, np.uint32)
+        self.lib.ref_tree_nodes(t, child, parent, cn, nu, lv)
+        return Tree(cm.reshape(-1, 4)[:count], child.reshape(n, 16), parent, cn, nu,
+                    self.lib.ref_tree_depth(t), bool(assoc))
+
+    def walk_seq(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
+                 diffusion: float = 1.0, use_cache: bool = True):
+        """Returns (out RgbaF, palette)."""
+        h, w = rgbaf.shape[:2]
+        px = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(px, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            count = self.lib.ref_tree_color_count(t)
+            cm = np.zeros(max(count, 1) * 4, np.float64)
+            self.lib.ref_tree_colormap(t, cm)
+            out = px.copy()
+            self.lib.ref_walk_seq(t, float(diffusion), int(use_cache), w, h, out)
+            return out.reshape(h, w, 4), cm.reshape(-1, 4)[:count]
+        finally:
+            self.lib.ref_tree_free(t)
+
+    def walk_blocks(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
+                    block: int, diffusion: float = 1.0):
+        h, w = rgbaf.shape[:2]
+        px = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(px, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            count = self.lib.ref_tree_color_count(t)
+            cm = np.zeros(max(count, 1) * 4, np.float64)
+            self.lib.ref_tree_colormap(t, cm)
+            out = px.copy()
+            err = C.create_string_buffer(1024)
+            rc = self.lib.ref_walk_blocks(t, float(diffusion), int(block), w, h, out, 1, err, 1024)
+            if rc != 0:
+                raise ValueError(err.value.decode())
+            return out.reshape(h, w, 4), cm.reshape(-1, 4)[:count]
+        finally:
+            self.lib.ref_tree_free(t)
+
+    def block_order(self, w: int, h: int):
+        out = np.empty(w * h + 1, np.int32)
+        owner = np.empty(max(w * h, 1), np.int32)
+        n = self.lib.ref_block_curve(w, h, out, owner)
+        return out[:n], owner[: w * h]
+
+    def curve_sequence(self, level: int) -> np.ndarray:
+        n = 1 << (2 * level)
+        xy = np.zeros(2 * n, np.int32)
+        self.lib.ref_curve_sequence(level, xy)
+        return xy.reshape(n, 2)
+
+    def error_weights(self) -> np.ndarray:
+        w = np.zeros(16, np.float64)
+        self.lib.ref_error_weights(w)
+        return w
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)

@@ -1,0 +1,373 @@
+"""Riemersma dithering on B200 (sm_100a): Python mirror of the C ABI in include/rdb.h.
+
+The engines live in ``stipple_b200/lib/librdb_b200.so`` (built by
+``python -m stipple_b200.build``).  This module only binds that library with
+ctypes for tests, the benchmark and scripting; it has no compute path of its
+own and raises if the library is missing.
+
+Engines (``ENGINE_*``) mirror the reference's entry points: ``SEQ`` is
+RiemersmaWalkCpu/Cuda (bit-exact, memoised), ``BLOCKS`` is
+RiemersmaBlocksCpu/Cuda (bit-exact with the host block walk), ``JACOBI`` is
+RiemersmaApproxCuda (tolerance-held).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "librdb_b200.so")
+
+RGB8, RGBA8, RGBAF32 = 3, 4, 16
+ENGINE_SEQ, ENGINE_BLOCKS, ENGINE_JACOBI = 0, 1, 2
+ENGINES = {"seq": ENGINE_SEQ, "blocks": ENGINE_BLOCKS, "jacobi": ENGINE_JACOBI}
+
+
+class RdbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rdb error {code}: {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("diffusion", C.c_double),
+        ("use_cache", C.c_int),
+        ("block", C.c_int),
+        ("jacobi_iters", C.c_int),
+        ("jacobi_taps", C.c_int),
+        ("jacobi_fp64", C.c_int),
+        ("cache_bits", C.c_int),
+        ("reserved", C.c_int * 8),
+    ]
+
+
+class Job(C.Structure):
+    _fields_ = [
+        ("pixels", C.c_void_p),
+        ("row_stride", C.c_size_t),
+        ("width", C.c_int),
+        ("height", C.c_int),
+        ("layout", C.c_int),
+        ("palette_id", C.c_int),
+        ("indices", C.c_void_p),
+        ("rgba_out", C.c_void_p),
+    ]
+
+
+HostJob = Job  # same layout: rdb_host_job
+
+
+class PaletteDesc(C.Structure):
+    _fields_ = [
+        ("count", C.c_int),
+        ("associate_alpha", C.c_int),
+        ("colors", C.c_void_p),
+        ("search_colors", C.c_void_p),
+        ("node_count", C.c_int),
+        ("root", C.c_int),
+        ("child", C.c_void_p),
+        ("parent", C.c_void_p),
+        ("color_number", C.c_void_p),
+        ("number_unique", C.c_void_p),
+    ]
+
+
+# Every symbol include/rdb.h declares, with (restype, argtypes).
+SIGNATURES = {
+    "rdb_last_error": (C.c_char_p, []),
+    "rdb_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "rdb_device_name": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t]),
+    "rdb_alloc_pinned": (C.c_void_p, [C.c_size_t]),
+    "rdb_free_pinned": (None, [C.c_void_p]),
+    "rdb_octree_build": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t,
+                                   C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "rdb_octree_color_count": (C.c_int, [C.c_void_p]),
+    "rdb_octree_node_count": (C.c_int, [C.c_void_p]),
+    "rdb_octree_depth": (C.c_int, [C.c_void_p]),
+    "rdb_octree_colormap": (None, [C.c_void_p, C.c_void_p]),
+    "rdb_octree_nodes": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rdb_octree_free": (None, [C.c_void_p]),
+    "rdb_is_grayscale": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t]),
+    "rdb_context_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "rdb_context_destroy": (None, [C.c_void_p]),
+    "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
+    "rdb_palette_create": (C.c_int, [C.c_void_p, C.POINTER(PaletteDesc), C.POINTER(C.c_int)]),
+    "rdb_palette_from_octree": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "rdb_plan_build": (C.c_int, [C.POINTER(PaletteDesc), C.c_void_p, C.c_size_t,
+                                 C.POINTER(C.c_size_t)]),
+    "rdb_palette_destroy": (C.c_int, [C.c_void_p, C.c_int]),
+    "rdb_options_default": (None, [C.POINTER(Options)]),
+    "rdb_dither": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Job), C.c_int, C.POINTER(Options),
+                             C.c_void_p]),
+    "rdb_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rdb_dither_host": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(HostJob), C.c_int,
+                                  C.POINTER(Options)]),
+    "rdb_error_weights": (None, [C.c_void_p]),
+    "rdb_inverse_filter": (C.c_int, [C.c_int, C.c_double, C.c_void_p]),
+    "rdb_block_gap": (C.c_int64, [C.c_int, C.c_int]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load librdb_b200.so; raises FileNotFoundError when it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m stipple_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RdbError(rc, load().rdb_last_error().decode())
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def options(**kw) -> Options:
+    o = Options()
+    load().rdb_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def layout_of(img: np.ndarray) -> int:
+    if img.dtype == np.float32:
+        if img.shape[-1] != 4:
+            raise ValueError("float images must be RGBA (Q16 RgbaF)")
+        return RGBAF32
+    if img.dtype != np.uint8 or img.shape[-1] not in (3, 4):
+        raise ValueError("uint8 images must be RGB or RGBA")
+    return int(img.shape[-1])
+
+
+class Octree:
+    """Host palette build with ImageMagick octree semantics (rdb_octree_build)."""
+
+    def __init__(self, img: np.ndarray, max_colors: int, associate_alpha: bool | None = None,
+                 grayscale: bool | None = None):
+        lib = load()
+        img = np.ascontiguousarray(img)
+        lay = layout_of(img)
+        h, w = img.shape[:2]
+        if associate_alpha is None:
+            associate_alpha = lay == RGBA8
+        if grayscale is None:
+            grayscale = bool(lib.rdb_is_grayscale(_ptr(img), lay, w, h, 0))
+        self.handle = C.c_void_p()
+        _check(lib.rdb_octree_build(_ptr(img), lay, w, h, 0, int(max_colors),
+                                    int(associate_alpha), int(grayscale), C.byref(self.handle)))
+        self.associate_alpha = bool(associate_alpha)
+        self.grayscale = bool(grayscale)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.rdb_octree_free(self.handle)
+            self.handle = None
+
+    @property
+    def count(self) -> int:
+        return load().rdb_octree_color_count(self.handle)
+
+    @property
+    def depth(self) -> int:
+        return load().rdb_octree_depth(self.handle)
+
+    def colormap(self) -> np.ndarray:
+        out = np.zeros((max(self.count, 1), 4), np.float64)
+        load().rdb_octree_colormap(self.handle, _ptr(out))
+        return out[: self.count]
+
+    def nodes(self):
+        n = load().rdb_octree_node_count(self.handle)
+        child = np.zeros((n, 16), np.int32)
+        parent = np.zeros(n, np.int32)
+        cn = np.zeros(n, np.uint32)
+        nu = np.zeros(n, np.uint64)
+        load().rdb_octree_nodes(self.handle, _ptr(child), _ptr(parent), _ptr(cn), _ptr(nu))
+        return child, parent, cn, nu
+
+
+class Context:
+    """A device context (rdb_context): resident palettes, orders, memo slabs."""
+
+    def __init__(self, device: int = 0, budget: int = 0):
+        lib = load()
+        self.handle = C.c_void_p()
+        _check(lib.rdb_context_create(device, budget, C.byref(self.handle)))
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            load().rdb_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.rdb_context_destroy(self.handle)
+            self.handle = None
+
+    @property
+    def bytes(self) -> int:
+        return load().rdb_context_bytes(self.handle)
+
+    # -- palettes ---------------------------------------------------------
+    def palette_from_octree(self, tree: Octree) -> int:
+        pid = C.c_int()
+        _check(load().rdb_palette_from_octree(self.handle, tree.handle, C.byref(pid)))
+        return pid.value
+
+    def palette(self, colors: np.ndarray, child: np.ndarray, color_number: np.ndarray,
+                number_unique: np.ndarray, associate_alpha: bool,
+                parent: np.ndarray | None = None, search_colors: np.ndarray | None = None,
+                root: int = 0) -> int:
+        d, keep = _desc(colors, child, color_number, number_unique, associate_alpha, parent,
+                        search_colors, root)
+        pid = C.c_int()
+        _check(load().rdb_palette_create(self.handle, C.byref(d), C.byref(pid)))
+        del keep
+        return pid.value
+
+    def palette_from_image(self, img: np.ndarray, max_colors: int, **kw) -> int:
+        return self.palette_from_octree(Octree(img, max_colors, **kw))
+
+    def release_palette(self, pid: int) -> None:
+        _check(load().rdb_palette_destroy(self.handle, pid))
+
+    # -- dithering (host buffers) ----------------------------------------
+    def dither_host(self, engine: str | int, images, palette_ids, rgba: bool = False,
+                    **opts):
+        """Dithers host images; returns a list of index maps (and RgbaF results)."""
+        eng = ENGINES[engine] if isinstance(engine, str) else engine
+        if isinstance(images, np.ndarray):
+            images, palette_ids = [images], [palette_ids]
+            single = True
+        else:
+            single = False
+        n = len(images)
+        jobs = (HostJob * n)()
+        outs, rgbs, keep = [], [], []
+        for i, (img, pid) in enumerate(zip(images, palette_ids)):
+            img = np.ascontiguousarray(img)
+            keep.append(img)
+            h, w = img.shape[:2]
+            idx = np.zeros((h, w), np.uint8)
+            outs.append(idx)
+            jobs[i].pixels = _ptr(img)
+            jobs[i].row_stride = 0
+            jobs[i].width = w
+            jobs[i].height = h
+            jobs[i].layout = layout_of(img)
+            jobs[i].palette_id = pid
+            jobs[i].indices = _ptr(idx)
+            if rgba:
+                r = np.zeros((h, w, 4), np.float32)
+                rgbs.append(r)
+                jobs[i].rgba_out = _ptr(r)
+        o = options(**opts)
+        _check(load().rdb_dither_host(self.handle, eng, jobs, n, C.byref(o)))
+        if single:
+            return (outs[0], rgbs[0]) if rgba else outs[0]
+        return (outs, rgbs) if rgba else outs
+
+    # -- dithering (device buffers; torch tensors as plumbing) ------------
+    def dither(self, engine: str | int, jobs: list[dict], stream: int = 0, **opts) -> None:
+        """Enqueue jobs whose buffers are device pointers: dicts with keys
+        pixels, width, height, layout, palette_id, indices, optional rgba_out
+        and row_stride."""
+        eng = ENGINES[engine] if isinstance(engine, str) else engine
+        n = len(jobs)
+        arr = (Job * n)()
+        for i, j in enumerate(jobs):
+            arr[i].pixels = j["pixels"]
+            arr[i].row_stride = j.get("row_stride", 0)
+            arr[i].width = j["width"]
+            arr[i].height = j["height"]
+            arr[i].layout = j["layout"]
+            arr[i].palette_id = j["palette_id"]
+            arr[i].indices = j["indices"]
+            arr[i].rgba_out = j.get("rgba_out") or 0
+        o = options(**opts)
+        _check(load().rdb_dither(self.handle, eng, arr, n, C.byref(o), stream or None))
+
+    def synchronize(self, stream: int = 0) -> None:
+        _check(load().rdb_synchronize(self.handle, stream or None))
+
+
+def _desc(colors, child, color_number, number_unique, associate_alpha, parent=None,
+          search_colors=None, root=0):
+    colors = np.ascontiguousarray(colors, np.float64)
+    child = np.ascontiguousarray(child, np.int32)
+    cn = np.ascontiguousarray(color_number, np.uint32)
+    nu = np.ascontiguousarray(number_unique, np.uint64)
+    keep = [colors, child, cn, nu]
+    d = PaletteDesc()
+    d.count = colors.shape[0]
+    d.associate_alpha = int(associate_alpha)
+    d.colors = _ptr(colors)
+    if search_colors is not None:
+        sc = np.ascontiguousarray(search_colors, np.float64)
+        keep.append(sc)
+        d.search_colors = _ptr(sc)
+    d.node_count = child.shape[0]
+    d.root = root
+    d.child = _ptr(child)
+    if parent is not None:
+        par = np.ascontiguousarray(parent, np.int32)
+        keep.append(par)
+        d.parent = _ptr(par)
+    d.color_number = _ptr(cn)
+    d.number_unique = _ptr(nu)
+    return d, keep
+
+
+def plan_blob(colors, child, color_number, number_unique, associate_alpha, parent=None,
+              search_colors=None, root=0) -> bytes:
+    """The device plan for a palette (rdb_plan_build), built on the host."""
+    d, keep = _desc(colors, child, color_number, number_unique, associate_alpha, parent,
+                    search_colors, root)
+    size = C.c_size_t()
+    _check(load().rdb_plan_build(C.byref(d), None, 0, C.byref(size)))
+    buf = np.zeros(size.value, np.uint8)
+    _check(load().rdb_plan_build(C.byref(d), _ptr(buf), size.value, C.byref(size)))
+    del keep
+    return buf.tobytes()
+
+
+def device_count() -> int:
+    c = C.c_int()
+    rc = load().rdb_device_count(C.byref(c))
+    return c.value if rc == 0 else 0
+
+
+def error_weights() -> np.ndarray:
+    w = np.zeros(16, np.float64)
+    load().rdb_error_weights(_ptr(w))
+    return w
+
+
+def inverse_filter(taps: int, diffusion: float = 1.0) -> np.ndarray:
+    g = np.zeros(taps + 1, np.float64)
+    _check(load().rdb_inverse_filter(taps, diffusion, _ptr(g)))
+    return g
+
+
+def block_gap(width: int, height: int) -> int:
+    return int(load().rdb_block_gap(width, height))

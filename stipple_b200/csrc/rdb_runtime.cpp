@@ -1,0 +1,563 @@
+// rdb_runtime.cpp -- host runtime of the engines (see rdb_runtime.h).
+#include "rdb_runtime.h"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "rdb_curve.h"
+#include "rdb_numeric.h"
+
+namespace rdb {
+namespace {
+
+thread_local std::string g_error;
+
+constexpr std::size_t kMaxOrders = 1024;  // resident geometries before eviction
+
+std::size_t RowStride(const rdb_job& j) {
+  return j.row_stride ? j.row_stride : static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
+}
+
+}  // namespace
+
+std::size_t BytesPerPixel(int layout) { return layout == RDB_RGBAF32 ? 16 : static_cast<std::size_t>(layout); }
+
+void SetError(const std::string& msg) { g_error = msg; }
+const char* LastError() { return g_error.c_str(); }
+
+int Fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+int CudaFail(cudaError_t e, const char* what) {
+  return Fail(e == cudaErrorMemoryAllocation ? RDB_E_NOMEM : RDB_E_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+Context::~Context() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& p : plans_) cudaFree(p.second.dev);
+  for (auto& o : orders_) cudaFree(o.second);
+  for (DevBuf* b : {&memo_, &memo_gen_, &seq_items_, &counter_, &status_, &curve_scratch_,
+                    &block_images_, &block_offsets_, &block_cx_, &block_chosen_, &jac_cx_,
+                    &jac_q_, &jac_g_, &host_in_, &host_idx_, &host_rgba_}) {
+    Release(b);
+  }
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Context::Init(int device, std::size_t budget) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return Fail(RDB_E_CUDA, "no CUDA device available");
+  if (device < 0 || device >= count) return Fail(RDB_E_INVALID, "device index out of range");
+  device_ = device;
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return CudaFail(e, "cudaSetDevice");
+  cudaDeviceProp prop{};
+  if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) {
+    return CudaFail(e, "cudaGetDeviceProperties");
+  }
+  if (prop.major < 10) {
+    return Fail(RDB_E_CUDA, std::string("device ") + prop.name +
+                                " is not sm_100 class; this library is built for sm_100a only");
+  }
+  sm_count_ = prop.multiProcessorCount;
+  smem_optin_ = prop.sharedMemPerBlockOptin;
+  std::size_t free_b = 0, total_b = 0;
+  if ((e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess) return CudaFail(e, "cudaMemGetInfo");
+  budget_ = budget ? budget : (free_b / 10) * 9;
+  if ((e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking)) != cudaSuccess) {
+    return CudaFail(e, "cudaStreamCreate");
+  }
+  if (Reserve(&counter_, 256, "work counter") || Reserve(&status_, 256, "status word")) {
+    return RDB_E_NOMEM;
+  }
+  cudaMemset(status_.ptr, 0, 256);
+  return RDB_OK;
+}
+
+void Context::Release(DevBuf* b) {
+  if (b->ptr) {
+    cudaFree(b->ptr);
+    bytes_ -= b->bytes;
+  }
+  b->ptr = nullptr;
+  b->bytes = 0;
+}
+
+int Context::Reserve(DevBuf* b, std::size_t bytes, const char* what) {
+  if (b->bytes >= bytes) return RDB_OK;
+  // Grow geometrically so a stream of slightly larger jobs does not thrash.
+  std::size_t want = std::max(bytes, b->bytes + b->bytes / 2);
+  if (bytes_ - b->bytes + want > budget_) want = bytes;
+  if (bytes_ - b->bytes + want > budget_) {
+    return Fail(RDB_E_NOMEM, std::string(what) + ": device memory budget exceeded");
+  }
+  if (b->ptr) {
+    // Every stream that may still read the old buffer must be done with it.
+    cudaDeviceSynchronize();
+  }
+  Release(b);
+  void* p = nullptr;
+  const cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) return CudaFail(e, what);
+  b->ptr = p;
+  b->bytes = want;
+  bytes_ += want;
+  return RDB_OK;
+}
+
+int Context::CreatePalette(const PlanInput& in, int* id) {
+  DevPlan p;
+  const std::string err = BuildPlan(in, &p.host);
+  if (!err.empty()) return Fail(RDB_E_UNSUPPORTED, err);
+  const PlanHeader* h = reinterpret_cast<const PlanHeader*>(p.host.data());
+  p.smem = h->smem_bytes;
+  p.count = h->count;
+  p.assoc = h->assoc != 0;
+  if (bytes_ + p.host.size() > budget_) return Fail(RDB_E_NOMEM, "palette: budget exceeded");
+  cudaError_t e = cudaMalloc(&p.dev, p.host.size());
+  if (e != cudaSuccess) return CudaFail(e, "palette upload");
+  e = cudaMemcpy(p.dev, p.host.data(), p.host.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(p.dev);
+    return CudaFail(e, "palette upload");
+  }
+  bytes_ += p.host.size();
+  const int pid = next_palette_++;
+  plans_[pid] = std::move(p);
+  *id = pid;
+  return RDB_OK;
+}
+
+int Context::DestroyPalette(int id) {
+  auto it = plans_.find(id);
+  if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
+  cudaStreamSynchronize(stream_);
+  cudaFree(it->second.dev);
+  bytes_ -= it->second.host.size();
+  plans_.erase(it);
+  return RDB_OK;
+}
+
+const DevPlan* Context::Plan(int id) const {
+  auto it = plans_.find(id);
+  return it == plans_.end() ? nullptr : &it->second;
+}
+
+int Context::Order(int width, int height, cudaStream_t s, const int32_t** out) {
+  const auto key = std::make_pair(width, height);
+  auto it = orders_.find(key);
+  if (it != orders_.end()) {
+    *out = it->second;
+    return RDB_OK;
+  }
+  const std::size_t n = static_cast<std::size_t>(width) * height;
+  const std::size_t bytes = std::max<std::size_t>(n, 1) * sizeof(int32_t);
+  while ((orders_.size() >= kMaxOrders || bytes_ + bytes > budget_) && !order_lru_.empty()) {
+    // Evict the oldest geometry (after the device is done with it).
+    cudaDeviceSynchronize();
+    const auto victim = order_lru_.front();
+    order_lru_.erase(order_lru_.begin());
+    auto v = orders_.find(victim);
+    if (v != orders_.end()) {
+      cudaFree(v->second);
+      bytes_ -= std::max<std::size_t>(static_cast<std::size_t>(victim.first) * victim.second, 1) *
+                sizeof(int32_t);
+      orders_.erase(v);
+    }
+  }
+  if (bytes_ + bytes > budget_) return Fail(RDB_E_NOMEM, "visit order: budget exceeded");
+  int32_t* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, bytes);
+  if (e != cudaSuccess) return CudaFail(e, "visit order allocation");
+  bytes_ += bytes;
+  const int level = CurveLevel(width, height);
+  const std::size_t scratch = CurveScratchBytes(level);
+  if (int rc = Reserve(&curve_scratch_, scratch, "curve scratch")) {
+    cudaFree(d);
+    bytes_ -= bytes;
+    return rc;
+  }
+  e = BuildSeqOrder(width, height, d, curve_scratch_.ptr, curve_scratch_.bytes, s);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    bytes_ -= bytes;
+    return CudaFail(e, "visit order kernel");
+  }
+  orders_[key] = d;
+  order_lru_.push_back(key);
+  *out = d;
+  return RDB_OK;
+}
+
+int Context::CheckJob(const rdb_job& j) const {
+  if (j.width < 1 || j.height < 1) return Fail(RDB_E_INVALID, "image must be at least 1x1");
+  if (static_cast<int64_t>(j.width) * j.height >= (static_cast<int64_t>(1) << 31) - 1) {
+    return Fail(RDB_E_UNSUPPORTED, "image larger than 2^31 - 2 pixels");
+  }
+  if (j.layout != RDB_RGB8 && j.layout != RDB_RGBA8 && j.layout != RDB_RGBAF32) {
+    return Fail(RDB_E_INVALID, "unknown pixel layout");
+  }
+  if (!j.pixels || !j.indices) return Fail(RDB_E_INVALID, "null pixel or index buffer");
+  if (j.layout == RDB_RGBAF32 && (reinterpret_cast<uintptr_t>(j.pixels) & 15u)) {
+    return Fail(RDB_E_INVALID, "RgbaF pixels must be 16-byte aligned");
+  }
+  if (j.layout == RDB_RGBA8 && (reinterpret_cast<uintptr_t>(j.pixels) & 3u)) {
+    return Fail(RDB_E_INVALID, "RGBA8 pixels must be 4-byte aligned");
+  }
+  const std::size_t stride = RowStride(j);
+  if (stride < static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout)) {
+    return Fail(RDB_E_INVALID, "row stride shorter than a row");
+  }
+  if ((j.layout == RDB_RGBAF32 && stride % 16) || (j.layout == RDB_RGBA8 && stride % 4)) {
+    return Fail(RDB_E_INVALID, "row stride breaks pixel alignment");
+  }
+  if (j.rgba_out && (reinterpret_cast<uintptr_t>(j.rgba_out) & 15u)) {
+    return Fail(RDB_E_INVALID, "RgbaF output must be 16-byte aligned");
+  }
+  if (!Plan(j.palette_id)) return Fail(RDB_E_INVALID, "unknown palette id");
+  return RDB_OK;
+}
+
+int Context::Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o,
+                    cudaStream_t s) {
+  if (n < 0 || (n > 0 && !jobs)) return Fail(RDB_E_INVALID, "bad job list");
+  if (n == 0) return RDB_OK;
+  for (int i = 0; i < n; ++i) {
+    if (int rc = CheckJob(jobs[i])) return rc;
+  }
+  if (!s) s = stream_;
+  cudaSetDevice(device_);
+  switch (engine) {
+    case RDB_ENGINE_SEQ: return Seq(jobs, n, o, s);
+    case RDB_ENGINE_BLOCKS: return Blocks(jobs, n, o, s);
+    case RDB_ENGINE_JACOBI: return Jacobi(jobs, n, o, s);
+    default: return Fail(RDB_E_INVALID, "unknown engine");
+  }
+}
+
+int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  std::vector<SeqItem> items(static_cast<std::size_t>(n));
+  int plan_max = 0;
+  bool any_assoc = false;
+  for (int i = 0; i < n; ++i) {
+    const rdb_job& j = jobs[i];
+    const DevPlan* p = Plan(j.palette_id);
+    const int32_t* order = nullptr;
+    if (int rc = Order(j.width, j.height, s, &order)) return rc;
+    SeqItem& it = items[static_cast<std::size_t>(i)];
+    it.pixels = static_cast<const unsigned char*>(j.pixels);
+    it.row_stride = static_cast<int64_t>(RowStride(j));
+    it.width = j.width;
+    it.height = j.height;
+    it.layout = j.layout;
+    it.n = j.width * j.height;
+    it.order = order;
+    it.indices = j.indices;
+    it.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+    it.plan = p->dev;
+    it.plan_smem = p->smem;
+    it.pad = 0;
+    plan_max = std::max(plan_max, p->smem);
+    any_assoc = any_assoc || p->assoc;
+  }
+  // Longest walk first: the makespan is bounded below by it.
+  std::stable_sort(items.begin(), items.end(),
+                   [](const SeqItem& a, const SeqItem& b) { return a.n > b.n; });
+
+  const bool use_cache = o.use_cache != 0;
+  // One warp per CTA.  Several CTAs share an SM once the batch is larger than
+  // the SM count; shared memory is split between them.
+  const int per_sm = std::min(8, std::max(1, (n + sm_count_ - 1) / sm_count_));
+  const int grid = std::min(n, sm_count_ * per_sm);
+  const std::size_t ring = 96 * (sizeof(int32_t) + 16);
+  const std::size_t smem_cap = std::min<std::size_t>(smem_optin_, (228 * 1024) / per_sm - 1024);
+  int cache_bits = o.cache_bits;
+  if (use_cache && cache_bits == 0) {
+    cache_bits = 15;
+    while (cache_bits > 8 &&
+           plan_max + ring + (static_cast<std::size_t>(4) << cache_bits) > smem_cap) {
+      --cache_bits;
+    }
+  }
+  if (use_cache && (cache_bits < 1 || cache_bits > 20)) {
+    return Fail(RDB_E_INVALID, "cache_bits out of range");
+  }
+  const std::size_t smem = SeqSmemBytes(plan_max, cache_bits, use_cache);
+  if (smem > smem_optin_) return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
+
+  // Memo slabs: one per CTA, 2^18 keys (2^24 with alpha), generation-tagged.
+  const int64_t entries = any_assoc ? (int64_t{1} << 24) : (int64_t{1} << 18);
+  if (use_cache && (grid > memo_grid_ || entries > memo_entries_)) {
+    const int g = std::max(grid, memo_grid_);
+    const int64_t en = std::max(entries, memo_entries_);
+    cudaDeviceSynchronize();  // earlier walks may still read the old slabs
+    Release(&memo_);
+    Release(&memo_gen_);
+    memo_grid_ = 0;
+    memo_entries_ = 0;
+    if (int rc = Reserve(&memo_, static_cast<std::size_t>(g) * en * sizeof(uint16_t), "memo slabs")) {
+      return rc;
+    }
+    if (int rc = Reserve(&memo_gen_, static_cast<std::size_t>(g) * sizeof(uint32_t), "memo generations")) {
+      return rc;
+    }
+    cudaMemsetAsync(memo_.ptr, 0, memo_.bytes, s);
+    cudaMemsetAsync(memo_gen_.ptr, 0, memo_gen_.bytes, s);
+    memo_grid_ = g;
+    memo_entries_ = en;
+  }
+  if (int rc = Reserve(&seq_items_, items.size() * sizeof(SeqItem), "work items")) return rc;
+  cudaError_t e = cudaMemcpyAsync(seq_items_.ptr, items.data(), items.size() * sizeof(SeqItem),
+                                  cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return CudaFail(e, "work item upload");
+  // The host vector must outlive the async copy.
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return CudaFail(e, "work item upload");
+  cudaMemsetAsync(counter_.ptr, 0, sizeof(int), s);
+
+  SeqLaunch L{};
+  L.items = static_cast<const SeqItem*>(seq_items_.ptr);
+  L.n_items = n;
+  L.work_counter = static_cast<int*>(counter_.ptr);
+  L.memo = static_cast<uint16_t*>(memo_.ptr);
+  L.memo_gen = static_cast<uint32_t*>(memo_gen_.ptr);
+  L.slab_entries = memo_entries_;
+  L.cache_bits = use_cache ? cache_bits : 0;
+  L.plan_smem_max = plan_max;
+  L.use_cache = use_cache ? 1 : 0;
+  scaled_weights(o.diffusion, L.sw);
+  L.status = static_cast<int*>(status_.ptr);
+  e = LaunchSeqWalk(L, grid, s);
+  if (e != cudaSuccess) return CudaFail(e, "sequential walk launch");
+  return RDB_OK;
+}
+
+int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  if (o.block < kQueue) {
+    return Fail(RDB_E_UNSUPPORTED, "--blocks must be at least 16 (the error queue is 16 entries deep)");
+  }
+  const int pid = jobs[0].palette_id;
+  const int layout = jobs[0].layout;
+  for (int i = 1; i < n; ++i) {
+    if (jobs[i].palette_id != pid || jobs[i].layout != layout) {
+      return Fail(RDB_E_INVALID, "blocks engine: one palette and one layout per call");
+    }
+  }
+  const DevPlan* p = Plan(pid);
+  std::vector<BlockImage> imgs;
+  std::vector<int64_t> offs;
+  int64_t blocks = 0, positions = 0;
+  for (int i = 0; i < n; ++i) {
+    const rdb_job& j = jobs[i];
+    const int64_t nb = BlockListLength(j.width, j.height);
+    if (nb == 0) {
+      // 1x1: BuildCurveIndex is empty and the pixel keeps its value.
+      if (j.rgba_out && j.rgba_out != j.pixels) {
+        const cudaError_t e = LaunchCopySource(static_cast<const unsigned char*>(j.pixels),
+                                               static_cast<int64_t>(RowStride(j)), j.width,
+                                               j.height, j.layout,
+                                               reinterpret_cast<float4*>(j.rgba_out), s);
+        if (e != cudaSuccess) return CudaFail(e, "source copy");
+      }
+      continue;
+    }
+    const int32_t* order = nullptr;
+    if (int rc = Order(j.width, j.height, s, &order)) return rc;
+    BlockImage b{};
+    b.pixels = static_cast<const unsigned char*>(j.pixels);
+    b.row_stride = static_cast<int64_t>(RowStride(j));
+    b.width = j.width;
+    b.height = j.height;
+    b.layout = j.layout;
+    b.n = static_cast<int>(nb);
+    b.order = order;
+    b.indices = j.indices;
+    b.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+    b.first_block = blocks;
+    b.nblocks = static_cast<int>((nb + o.block - 1) / o.block);
+    blocks += b.nblocks;
+    offs.push_back(positions);
+    positions += (nb + 15) & ~int64_t{15};
+    imgs.push_back(b);
+  }
+  if (imgs.empty()) return RDB_OK;
+  const std::size_t word = layout == RDB_RGBAF32 ? 16 : 4;
+  if (int rc = Reserve(&block_images_, imgs.size() * sizeof(BlockImage), "block images")) return rc;
+  if (int rc = Reserve(&block_offsets_, offs.size() * sizeof(int64_t), "block offsets")) return rc;
+  if (int rc = Reserve(&block_cx_, static_cast<std::size_t>(positions) * word, "block samples")) return rc;
+  if (int rc = Reserve(&block_chosen_, static_cast<std::size_t>(positions), "block indices")) return rc;
+  cudaMemcpyAsync(block_images_.ptr, imgs.data(), imgs.size() * sizeof(BlockImage),
+                  cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(block_offsets_.ptr, offs.data(), offs.size() * sizeof(int64_t),
+                  cudaMemcpyHostToDevice, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return CudaFail(e, "block descriptor upload");
+  BlockLaunch L{};
+  L.images = static_cast<const BlockImage*>(block_images_.ptr);
+  L.n_images = static_cast<int>(imgs.size());
+  L.block = o.block;
+  L.total_blocks = blocks;
+  L.cx = static_cast<uint32_t*>(block_cx_.ptr);
+  L.chosen = static_cast<uint8_t*>(block_chosen_.ptr);
+  L.cx_offset = static_cast<int64_t*>(block_offsets_.ptr);
+  L.plan = p->dev;
+  L.plan_smem = p->smem;
+  scaled_weights(o.diffusion, L.sw);
+  L.status = static_cast<int*>(status_.ptr);
+  e = LaunchBlockWalk(L, positions, s);
+  if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
+  return RDB_OK;
+}
+
+int Context::Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  if (o.jacobi_taps < 1 || o.jacobi_taps > 4096) return Fail(RDB_E_UNSUPPORTED, "--approx-taps out of range");
+  if (o.jacobi_iters < 0) return Fail(RDB_E_INVALID, "negative Jacobi iteration count");
+  std::vector<double> g(static_cast<std::size_t>(o.jacobi_taps) + 1);
+  {
+    double w[kQueue];
+    error_weights(w);
+    g[0] = 1.0;
+    for (int d = 1; d <= o.jacobi_taps; ++d) {
+      double acc = 0.0;
+      const int kmax = d < kQueue ? d : kQueue;
+      for (int k = 1; k <= kmax; ++k) acc += (o.diffusion / 16.0) * w[k - 1] * g[d - k];
+      g[d] = acc;
+    }
+  }
+  if (int rc = Reserve(&jac_g_, g.size() * sizeof(double), "filter")) return rc;
+  cudaMemcpyAsync(jac_g_.ptr, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return CudaFail(e, "filter upload");
+  for (int i = 0; i < n; ++i) {
+    const rdb_job& j = jobs[i];
+    const int64_t nb = BlockListLength(j.width, j.height);
+    if (nb == 0) {
+      if (j.rgba_out && j.rgba_out != j.pixels) {
+        e = LaunchCopySource(static_cast<const unsigned char*>(j.pixels),
+                             static_cast<int64_t>(RowStride(j)), j.width, j.height, j.layout,
+                             reinterpret_cast<float4*>(j.rgba_out), s);
+        if (e != cudaSuccess) return CudaFail(e, "source copy");
+      }
+      continue;
+    }
+    const DevPlan* p = Plan(j.palette_id);
+    const int32_t* order = nullptr;
+    if (int rc = Order(j.width, j.height, s, &order)) return rc;
+    const std::size_t elem = o.jacobi_fp64 ? sizeof(double) : sizeof(float);
+    if (int rc = Reserve(&jac_cx_, static_cast<std::size_t>(nb) * 4 * elem, "Jacobi samples")) return rc;
+    if (int rc = Reserve(&jac_q_, static_cast<std::size_t>(nb) * 2 + 64, "Jacobi indices")) return rc;
+    JacobiLaunch L{};
+    L.pixels = static_cast<const unsigned char*>(j.pixels);
+    L.row_stride = static_cast<int64_t>(RowStride(j));
+    L.width = j.width;
+    L.height = j.height;
+    L.layout = j.layout;
+    L.n = static_cast<int>(nb);
+    L.order = order;
+    L.indices = j.indices;
+    L.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+    L.plan = p->dev;
+    L.plan_smem = p->smem;
+    L.iterations = o.jacobi_iters;
+    L.taps = o.jacobi_taps;
+    L.fp64 = o.jacobi_fp64;
+    L.cx = jac_cx_.ptr;
+    L.q0 = static_cast<uint8_t*>(jac_q_.ptr);
+    L.q1 = L.q0 + ((nb + 31) & ~int64_t{31});
+    L.g = static_cast<const double*>(jac_g_.ptr);
+    L.status = static_cast<int*>(status_.ptr);
+    e = LaunchJacobi(L, s);
+    if (e != cudaSuccess) return CudaFail(e, "Jacobi launch");
+  }
+  return RDB_OK;
+}
+
+int Context::Synchronize(cudaStream_t s) {
+  if (!s) s = stream_;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return CudaFail(e, "kernel execution");
+  int status = 0;
+  e = cudaMemcpy(&status, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return CudaFail(e, "status readback");
+  if (status != 0) {
+    cudaMemset(status_.ptr, 0, sizeof(int));
+    return Fail(RDB_E_DEVICE, "a kernel reported status " + std::to_string(status));
+  }
+  return RDB_OK;
+}
+
+int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_options& o) {
+  if (n <= 0) return n == 0 ? RDB_OK : Fail(RDB_E_INVALID, "bad job list");
+  // Stage every job's input back to back (256-byte aligned slices).
+  std::vector<std::size_t> in_off(static_cast<std::size_t>(n)), idx_off(static_cast<std::size_t>(n)),
+      rgba_off(static_cast<std::size_t>(n));
+  std::size_t in_total = 0, idx_total = 0, rgba_total = 0;
+  const auto al = [](std::size_t v) { return (v + 255) & ~static_cast<std::size_t>(255); };
+  for (int i = 0; i < n; ++i) {
+    const rdb_host_job& j = jobs[i];
+    if (j.width < 1 || j.height < 1 || !j.pixels || !j.indices) {
+      return Fail(RDB_E_INVALID, "bad host job");
+    }
+    const std::size_t row = static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
+    in_off[i] = in_total;
+    in_total = al(in_total + row * j.height);
+    idx_off[i] = idx_total;
+    idx_total = al(idx_total + static_cast<std::size_t>(j.width) * j.height);
+    rgba_off[i] = rgba_total;
+    if (j.rgba_out) rgba_total = al(rgba_total + static_cast<std::size_t>(j.width) * j.height * 16);
+  }
+  if (int rc = Reserve(&host_in_, in_total, "input staging")) return rc;
+  if (int rc = Reserve(&host_idx_, idx_total, "index staging")) return rc;
+  if (rgba_total && Reserve(&host_rgba_, rgba_total, "RgbaF staging")) return RDB_E_NOMEM;
+  cudaStream_t s = stream_;
+  cudaSetDevice(device_);
+  std::vector<rdb_job> dj(static_cast<std::size_t>(n));
+  for (int i = 0; i < n; ++i) {
+    const rdb_host_job& j = jobs[i];
+    const std::size_t row = static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
+    unsigned char* din = static_cast<unsigned char*>(host_in_.ptr) + in_off[i];
+    cudaError_t e;
+    if (j.row_stride == 0 || j.row_stride == row) {
+      e = cudaMemcpyAsync(din, j.pixels, row * j.height, cudaMemcpyHostToDevice, s);
+    } else {
+      e = cudaMemcpy2DAsync(din, row, j.pixels, j.row_stride, row, j.height,
+                            cudaMemcpyHostToDevice, s);
+    }
+    if (e != cudaSuccess) return CudaFail(e, "input upload");
+    rdb_job& d = dj[static_cast<std::size_t>(i)];
+    d.pixels = din;
+    d.row_stride = row;
+    d.width = j.width;
+    d.height = j.height;
+    d.layout = j.layout;
+    d.palette_id = j.palette_id;
+    d.indices = static_cast<uint8_t*>(host_idx_.ptr) + idx_off[i];
+    // RgbaF results follow the reference's in-place semantics: an RgbaF input
+    // is dithered in place, so a pixel no engine writes keeps its source.
+    d.rgba_out = !j.rgba_out ? nullptr
+                 : j.layout == RDB_RGBAF32
+                     ? reinterpret_cast<float*>(din)
+                     : reinterpret_cast<float*>(static_cast<unsigned char*>(host_rgba_.ptr) +
+                                                rgba_off[i]);
+  }
+  // Cells an engine leaves unwritten (the block list's gap) read back as 0.
+  cudaMemsetAsync(host_idx_.ptr, 0, idx_total, s);
+  if (int rc = Dither(engine, dj.data(), n, o, s)) return rc;
+  for (int i = 0; i < n; ++i) {
+    const rdb_host_job& j = jobs[i];
+    const std::size_t npx = static_cast<std::size_t>(j.width) * j.height;
+    cudaError_t e = cudaMemcpyAsync(j.indices, dj[i].indices, npx, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return CudaFail(e, "index download");
+    if (j.rgba_out) {
+      e = cudaMemcpyAsync(j.rgba_out, dj[i].rgba_out, npx * 16, cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return CudaFail(e, "RgbaF download");
+    }
+  }
+  return Synchronize(s);
+}
+
+}  // namespace rdb

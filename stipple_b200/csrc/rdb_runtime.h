@@ -1,0 +1,110 @@
+// rdb_runtime.h -- the host runtime behind the C ABI: one device context with
+// resident palettes, per-geometry visit orders, memo slabs and scratch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/rdb.h"
+#include "rdb_plan.h"
+#include "rdb_walk.h"
+
+namespace rdb {
+
+// Thread-local error message (rdb_last_error).
+void SetError(const std::string& msg);
+const char* LastError();
+std::size_t BytesPerPixel(int layout);
+int Fail(int code, const std::string& msg);
+int CudaFail(cudaError_t e, const char* what);
+
+// A device buffer that only grows.
+struct DevBuf {
+  void* ptr = nullptr;
+  std::size_t bytes = 0;
+};
+
+struct DevPlan {
+  unsigned char* dev = nullptr;
+  std::vector<uint8_t> host;
+  int smem = 0;
+  int count = 0;
+  bool assoc = false;
+};
+
+class Context {
+ public:
+  ~Context();
+  int Init(int device, std::size_t budget);
+
+  int CreatePalette(const PlanInput& in, int* id);
+  int DestroyPalette(int id);
+  const DevPlan* Plan(int id) const;
+
+  // Visit order of a geometry, built on first use and kept resident.
+  int Order(int width, int height, cudaStream_t s, const int32_t** out);
+
+  int Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_options& o);
+  int Synchronize(cudaStream_t s);
+
+  std::size_t bytes() const { return bytes_; }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+  int sm_count() const { return sm_count_; }
+
+  // Grows `b` to at least `bytes`; frees and reallocates (contents lost).
+  int Reserve(DevBuf* b, std::size_t bytes, const char* what);
+
+ private:
+  int Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int CheckJob(const rdb_job& j) const;
+  void Release(DevBuf* b);
+
+  int device_ = 0;
+  int sm_count_ = 148;
+  std::size_t smem_optin_ = 227 * 1024;
+  std::size_t budget_ = 0;
+  std::size_t bytes_ = 0;
+  cudaStream_t stream_ = nullptr;
+  int next_palette_ = 1;
+  std::map<int, DevPlan> plans_;
+  std::map<std::pair<int, int>, int32_t*> orders_;
+  std::vector<std::pair<int, int>> order_lru_;
+
+  // Sequential engine state.
+  DevBuf memo_;
+  DevBuf memo_gen_;
+  int memo_grid_ = 0;
+  int64_t memo_entries_ = 0;
+  DevBuf seq_items_;
+  DevBuf counter_;
+  DevBuf status_;
+  // Blocks / Jacobi scratch.
+  DevBuf curve_scratch_;
+  DevBuf block_images_;
+  DevBuf block_offsets_;
+  DevBuf block_cx_;
+  DevBuf block_chosen_;
+  DevBuf jac_cx_;
+  DevBuf jac_q_;
+  DevBuf jac_g_;
+  // Host-form staging.
+  DevBuf host_in_;
+  DevBuf host_idx_;
+  DevBuf host_rgba_;
+};
+
+}  // namespace rdb
+
+struct rdb_context {
+  rdb::Context impl;
+};

@@ -1,0 +1,111 @@
+// rdb_walk.h -- launch descriptors shared by the engines and the host runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace rdb {
+
+// One image walked by the sequential-exact engine.
+struct SeqItem {
+  const unsigned char* pixels;  // device, row-major, `layout`
+  int64_t row_stride;           // bytes
+  int width;
+  int height;
+  int layout;                   // 3 = RGB8, 4 = RGBA8, 16 = RGBA float (Q16)
+  int n;                        // positions = width * height
+  const int32_t* order;         // visit order (pixel indices), n entries
+  uint8_t* indices;             // palette index per pixel, row-major
+  float4* rgba_out;             // optional RgbaF result (may alias `pixels` for layout 16)
+  const unsigned char* plan;    // device plan blob (rdb_plan.h)
+  int plan_smem;                // PlanHeader::smem_bytes
+  int pad;
+};
+
+struct SeqLaunch {
+  const SeqItem* items;
+  int n_items;
+  int* work_counter;            // zero before launch
+  uint16_t* memo;               // grid x slab_entries, generation-tagged
+  uint32_t* memo_gen;           // per CTA: last generation used in its slab
+  int64_t slab_entries;         // 2^18, or 2^24 when any item associates alpha
+  int cache_bits;               // log2 of the shared-memory memo cache entries
+  int plan_smem_max;            // bytes reserved for a plan in shared memory
+  int use_cache;                // 0: --no-cache, every lookup searched
+  int pad;
+  double sw[16];                // scaled error weights
+  int* status;
+};
+
+std::size_t SeqSmemBytes(int plan_smem_max, int cache_bits, bool use_cache);
+cudaError_t LaunchSeqWalk(const SeqLaunch& L, int grid, cudaStream_t stream);
+
+// The block engine: every image is cut into blocks of `block` consecutive
+// positions of the block-mode list, each walked from a zeroed queue with no
+// memo (src/rd_riemersma_cpu.cpp:632-697).
+struct BlockImage {
+  const unsigned char* pixels;
+  int64_t row_stride;
+  int width;
+  int height;
+  int layout;
+  int n;                        // block-list length (BlockListLength)
+  const int32_t* order;         // sequential order of the geometry (W*H entries)
+  uint8_t* indices;             // palette index per pixel, row-major
+  float4* rgba_out;             // optional RgbaF result
+  int64_t first_block;          // prefix over images
+  int nblocks;
+  int pad;
+};
+
+struct BlockLaunch {
+  const BlockImage* images;
+  int n_images;
+  int block;                    // positions per block (>= 16)
+  int64_t total_blocks;
+  uint32_t* cx;                 // scratch: curve-ordered samples (one word per position)
+  uint8_t* chosen;              // scratch: index per curve position
+  int64_t* cx_offset;           // per image: offset of its curve positions in cx/chosen
+  const unsigned char* plan;    // one palette for the launch
+  int plan_smem;
+  int pad;
+  double sw[16];
+  int* status;
+};
+
+cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream);
+
+// Writes every pixel's source value, as RgbaF, into `out` -- the result an
+// engine that visits nothing leaves (a 1x1 image in block mode).
+cudaError_t LaunchCopySource(const unsigned char* pixels, int64_t stride, int width, int height,
+                             int layout, float4* out, cudaStream_t stream);
+
+// The Jacobi engine (src/rd_approx_cuda.cu): an order-free fixed-point
+// iteration t = q + F (x - q) along the block-mode list.
+struct JacobiLaunch {
+  const unsigned char* pixels;
+  int64_t row_stride;
+  int width;
+  int height;
+  int layout;
+  int n;                        // block-list length
+  const int32_t* order;
+  uint8_t* indices;
+  float4* rgba_out;
+  const unsigned char* plan;
+  int plan_smem;
+  int iterations;
+  int taps;
+  int fp64;
+  void* cx;                     // scratch: n x 4 samples (float or double)
+  uint8_t* q0;                  // scratch: n
+  uint8_t* q1;                  // scratch: n
+  const double* g;              // taps + 1 filter coefficients (device)
+  int* status;
+};
+
+cudaError_t LaunchJacobi(const JacobiLaunch& L, cudaStream_t stream);
+
+}  // namespace rdb

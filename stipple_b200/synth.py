@@ -1,0 +1,96 @@
+"""Seeded synthetic inputs for the Riemersma workloads.
+
+No public dataset is involved: every workload is generated from a seed.
+
+* RGB8: per channel, the sum of three 2-D sinusoid gradients
+  ``A_k * sin(2*pi*(fx*x + fy*y)/N + phi_k)`` with seeded amplitude, phase,
+  frequency and orientation, centred on mid-grey, plus Gaussian noise of a
+  given sigma; rounded and clamped to 0..255.
+* RGBA8: the same RGB plus an alpha channel that is 0 on a seeded Bernoulli
+  mask (about 20 % of pixels) and 255 elsewhere.
+* Video: the gradient phase advances by a fixed number of pixels per frame
+  (a translation) and each frame draws fresh noise.
+
+8-bit samples map to the Q16 range as ``v * 257``, the factor an 8-bit decode
+into ImageMagick's 16-bit quantum produces.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _waves(rng: np.random.Generator, channels: int):
+    out = []
+    for _ in range(channels):
+        ch = []
+        for _k in range(3):
+            amp = rng.uniform(25.0, 55.0)
+            phase = rng.uniform(0.0, 2.0 * math.pi)
+            theta = rng.uniform(0.0, 2.0 * math.pi)
+            cycles = rng.uniform(0.5, 3.0)
+            ch.append((amp, phase, math.cos(theta) * cycles, math.sin(theta) * cycles))
+        out.append(ch)
+    return out
+
+
+def gradient_rgb8(width: int, height: int, seed: int, sigma: float = 8.0,
+                  shift: float = 0.0, noise_seed: int | None = None) -> np.ndarray:
+    """(H, W, 3) uint8 gradient+noise image.  ``shift`` translates the gradients
+    by that many pixels along x (used for video frames)."""
+    rng = np.random.default_rng(seed)
+    waves = _waves(rng, 3)
+    n = float(max(width, height, 1))
+    xs = (np.arange(width, dtype=np.float64) - shift)[None, :]
+    ys = np.arange(height, dtype=np.float64)[:, None]
+    nrng = np.random.default_rng(seed if noise_seed is None else noise_seed)
+    img = np.empty((height, width, 3), np.uint8)
+    for c in range(3):
+        acc = np.full((height, width), 128.0)
+        for amp, phase, fx, fy in waves[c]:
+            acc += amp * np.sin(2.0 * math.pi * (fx * xs + fy * ys) / n + phase)
+        if sigma > 0:
+            acc += nrng.normal(0.0, sigma, size=(height, width))
+        img[:, :, c] = np.clip(np.rint(acc), 0, 255).astype(np.uint8)
+    return img
+
+
+def alpha_mask(width: int, height: int, seed: int, transparent: float = 0.2) -> np.ndarray:
+    rng = np.random.default_rng(seed ^ 0x5A5A5A5A)
+    return np.where(rng.random((height, width)) < transparent, 0, 255).astype(np.uint8)
+
+
+def gradient_rgba8(width: int, height: int, seed: int, sigma: float = 8.0,
+                   transparent: float = 0.2) -> np.ndarray:
+    rgb = gradient_rgb8(width, height, seed, sigma)
+    a = alpha_mask(width, height, seed, transparent)
+    return np.concatenate([rgb, a[:, :, None]], axis=2)
+
+
+def video_frame(width: int, height: int, seed: int, frame: int, sigma: float = 6.0,
+                px_per_frame: float = 2.0) -> np.ndarray:
+    return gradient_rgb8(width, height, seed, sigma, shift=px_per_frame * frame,
+                         noise_seed=seed * 100003 + frame + 1)
+
+
+def to_q16(img8: np.ndarray) -> np.ndarray:
+    """uint8 (H, W, 3|4) -> float32 (H, W, 4) Q16 RGBA, opaque when no alpha."""
+    h, w, c = img8.shape
+    out = np.empty((h, w, 4), np.float32)
+    out[:, :, :c] = img8.astype(np.float32) * np.float32(257.0)
+    if c == 3:
+        out[:, :, 3] = np.float32(65535.0)
+    return out
+
+
+def is_grayscale(img: np.ndarray) -> bool:
+    """The reference's greyscale rule: every pixel has r == g == b."""
+    return bool(np.all(img[..., 0] == img[..., 1]) and np.all(img[..., 1] == img[..., 2]))
+
+
+def log_uniform_sizes(n: int, seed: int, lo: int = 1, hi: int = 4096):
+    rng = np.random.default_rng(seed)
+    ws = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(int)
+    hs = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(int)
+    return [(int(max(lo, w)), int(max(lo, h))) for w, h in zip(ws, hs)]

@@ -1,0 +1,62 @@
+"""Jacobi (order-free) engine: held to a stated tolerance against the
+sequential walk, not to equality (src/rd_approx_cuda.cu converges to the
+cache-free fixed point; the memo table's first-touch order is out of reach
+of any order-free scheme)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import stipple_b200 as sb
+from stipple_b200 import metrics, synth
+
+pytestmark = pytest.mark.gpu
+
+# Measured tolerance of this engine (20 sweeps, 96 taps) on the synthetic
+# gradient+noise workload, against the cache-free and the memoised walks.
+MAX_MISMATCH_NOCACHE = 0.05
+MAX_MISMATCH_CACHED = 0.25
+MAX_DELTA_E = 3.0
+
+
+@pytest.mark.parametrize("colors,alpha", [(16, False), (64, False), (256, False), (16, True)])
+def test_jacobi_tolerance(ctx, oracle, colors, alpha):
+    img = synth.gradient_rgba8(320, 240, 21) if alpha else synth.gradient_rgb8(320, 240, 21)
+    t = sb.Octree(img, colors, alpha)
+    pid = ctx.palette_from_octree(t)
+    try:
+        got = ctx.dither_host("jacobi", img, pid)
+        q = synth.to_q16(img)
+        cached, _, pal = oracle.walk_seq(q, colors, alpha, t.grayscale)
+        free, _, _ = oracle.walk_seq(q, colors, alpha, t.grayscale, use_cache=False)
+        gap = sb.block_gap(*img.shape[1::-1])
+        mask = np.ones(got.size, bool)
+        if gap >= 0:
+            mask[gap] = False
+        g, c, f = got.reshape(-1)[mask], cached.reshape(-1)[mask], free.reshape(-1)[mask]
+        mm_free = metrics.index_mismatch(g, f)
+        mm_cached = metrics.index_mismatch(g, c)
+        de = metrics.mean_delta_e(pal, g, c)
+        print(f"jacobi colors={colors} alpha={alpha}: mismatch vs cache-free {mm_free:.4f}, "
+              f"vs memoised {mm_cached:.4f}, mean dE76 {de:.3f}")
+        assert mm_free <= MAX_MISMATCH_NOCACHE
+        assert mm_cached <= MAX_MISMATCH_CACHED
+        assert de <= MAX_DELTA_E
+    finally:
+        ctx.release_palette(pid)
+
+
+def test_jacobi_fp64_and_taps(ctx):
+    img = synth.gradient_rgb8(200, 150, 3)
+    t = sb.Octree(img, 16, False)
+    pid = ctx.palette_from_octree(t)
+    try:
+        a = ctx.dither_host("jacobi", img, pid)
+        b = ctx.dither_host("jacobi", img, pid, jacobi_fp64=1)
+        assert metrics.index_mismatch(a, b) < 0.02
+        c = ctx.dither_host("jacobi", img, pid, jacobi_taps=16, jacobi_iters=4)
+        assert c.shape == a.shape
+        with pytest.raises(sb.RdbError):
+            ctx.dither_host("jacobi", img, pid, jacobi_taps=0)
+    finally:
+        ctx.release_palette(pid)
