@@ -1,0 +1,372 @@
+"""Benchmark: Mpixel/s of the Riemersma engines on B200.
+
+Headline workload (`value`, `e2e`): the sequential-exact walk of one
+3840x2160 RGB8 frame, 256-colour octree palette, one image per launch (the
+plain GPU form), bit-exact with the reference CPU walk.  Synthetic seeded
+gradient+noise input (no dataset).  Each step is one full walk.
+
+Also measured and reported in the same JSON line:
+  blocks   the block engine on a 4K video batch (fixed palette), GB/s vs HBM
+  batched  512 uneven RGBA8 images in one persistent launch vs the plain
+           one-launch-per-image form (config 3), with the Amdahl cap
+  roofline, cpu_baseline, clocks, e2e, gpu_launches
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one process per GPU, launched by
+torch.distributed.run): the images are independent, nothing is exchanged.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HEADLINE = dict(width=3840, height=2160, colors=256, seed=1)
+METRIC = "Mpixel/s seq-exact & block engines @4K, batched vs plain; p50/p99 serve latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--block-frames", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--skip-extra", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- helpers
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_cores() -> int:
+    return os.cpu_count() or 1
+
+
+def reference_cpu(img8: np.ndarray, colors: int, budget_s: float):
+    """The reference's own RiemersmaWalkCpu (oracle/_ref) or, where that build is
+    absent, the C restatement, on the same frame; repeated up to `budget_s`."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from stipple_b200 import synth
+    q = synth.to_q16(img8)
+    kind = "reference"
+    try:
+        lib = pyoracle.RefLib()
+        run = lambda: lib.walk_seq(q, colors, False, False)  # noqa: E731
+    except FileNotFoundError:
+        kind = "port"
+        orc = pyoracle.Oracle()
+        run = lambda: orc.walk_seq(q, colors, False, False)  # noqa: E731
+    # Palette build is part of these calls; time it separately and subtract.
+    t0 = time.perf_counter()
+    if kind == "reference":
+        lib.build_tree(q, colors, False, False)
+    else:
+        orc.build_tree(q, colors, False, False)
+    t_tree = time.perf_counter() - t0
+    times = []
+    start = time.perf_counter()
+    while not times or (time.perf_counter() - start < budget_s and len(times) < 20):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0 - t_tree)
+    px = img8.shape[0] * img8.shape[1]
+    med = statistics.median(times)
+    return {"value": px / med / 1e6, "unit": "Mpixel/s", "cores": 1, "kind": kind,
+            "sample": f"{len(times)} sequential walks of the {img8.shape[1]}x{img8.shape[0]} frame "
+                      f"({colors} colours), median, palette build excluded"}, times
+
+
+# --------------------------------------------------------------- main arm
+def run_ours(a, rank: int, world: int):
+    import torch
+    import stipple_b200 as sb
+    from stipple_b200 import synth
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    ctx = sb.Context(dev)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    s = stream.cuda_stream
+    W, H, C = HEADLINE["width"], HEADLINE["height"], HEADLINE["colors"]
+    img = synth.gradient_rgb8(W, H, HEADLINE["seed"] + rank)
+    tree = sb.Octree(img, C, False, False)
+    pid = ctx.palette_from_octree(tree)
+    d_img = torch.from_numpy(img).cuda()
+    d_idx = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    job = dict(pixels=d_img.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
+               indices=d_idx.data_ptr())
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step_dev():
+        ctx.dither("seq", [job], stream=s)
+
+    for _ in range(a.warmup):
+        step_dev()
+    ctx.synchronize(s)
+    if world > 1:
+        torch.distributed.barrier()
+    times = []
+    with ClockSampler(dev) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_dev()
+            e1.record(stream)
+            ctx.synchronize(s)
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        torch.distributed.barrier()
+    px = W * H
+    value = world * px * a.steps / (total_ms / 1e3) / 1e6
+    ms_step = total_ms / a.steps
+
+    # Reference-facing call with host buffers: H2D + walk + D2H every step.
+    pinned_in = torch.from_numpy(img).pin_memory()
+    pinned_out = torch.empty((H, W), dtype=torch.uint8).pin_memory()
+    e2e_t = []
+    for k in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        ctx.dither_host_into("seq", pinned_in.numpy(), pid, pinned_out.numpy())
+        if k >= a.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e = {"value": world * px * len(e2e_t) / sum(e2e_t) / 1e6, "unit": "Mpixel/s",
+           "h2d_bytes_per_step": int(img.nbytes), "d2h_bytes_per_step": int(W * H)}
+
+    hbm, peak_kind = peaks()
+    alg_bytes = px * 4  # 3 B of RGB8 read + 1 B of index written per pixel
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "kernel": "SeqWalkKernel",
+                "note": "the sequential walk is a dependent chain: its real bound is "
+                        "the per-pixel chain latency, see chain"}
+    chain = {"ns_per_px": ms_step * 1e6 / px, "clock_mhz": clk.summary()["sm_mhz"]}
+    if chain["clock_mhz"]:
+        chain["cycles_per_px"] = chain["ns_per_px"] * chain["clock_mhz"] / 1e3
+
+    out = {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded gradient + noise sigma 8, RGB8)",
+           "config": {"workload": "seq-exact walk, one 3840x2160 RGB8 frame per launch, "
+                                  "256-colour octree palette, bit-exact",
+                      "width": W, "height": H, "colors": C, "palette_colors": tree.count,
+                      "l2": "flushed between timed steps (256 MB write)",
+                      "parallelism": f"replicas x{world}"},
+           "e2e": e2e, "roofline": roofline, "chain": chain, "clocks": clk.summary(),
+           "gpu_launches": a.steps}
+
+    if rank == 0 and not a.skip_extra:
+        out["blocks"] = bench_blocks(ctx, s, a, tree, pid, hbm)
+        out["batched"] = bench_batched(ctx, s, a)
+    if rank == 0:
+        cpu, _ = reference_cpu(img, C, budget_s=12.0)
+        out["cpu_baseline"] = cpu
+    ctx.release_palette(pid)
+    return out
+
+
+def bench_blocks(ctx, s, a, tree, pid, hbm):
+    import torch
+    import stipple_b200 as sb
+    from stipple_b200 import synth
+    W, H = HEADLINE["width"], HEADLINE["height"]
+    n = a.block_frames
+    frames = [torch.from_numpy(synth.video_frame(W, H, 3, f)).cuda() for f in range(n)]
+    outs = [torch.empty((H, W), dtype=torch.uint8, device="cuda") for _ in range(n)]
+    jobs = [dict(pixels=f.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
+                 indices=o.data_ptr()) for f, o in zip(frames, outs)]
+    res = {}
+    for B in (256, 512, 4096):
+        ctx.dither("blocks", jobs, stream=s, block=B)
+        ctx.synchronize(s)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.current_stream())
+        ctx.dither("blocks", jobs, stream=s, block=B)
+        e1.record(torch.cuda.current_stream())
+        ctx.synchronize(s)
+        ms = e0.elapsed_time(e1)
+        px = n * W * H
+        gbs = px * 4 / (ms / 1e3) / 1e9
+        res[f"B{B}"] = {"ms": ms, "mpx_s": px / ms / 1e3, "gb_s": gbs, "hbm_frac": gbs / hbm}
+    res["workload"] = f"{n} frames of 3840x2160 RGB8 video, fixed 256-colour palette"
+    return res
+
+
+def bench_batched(ctx, s, a):
+    import torch
+    import stipple_b200 as sb
+    from stipple_b200 import synth
+    sizes = synth.log_uniform_sizes(a.batch - 4, seed=2024) + [(1, 1), (3, 5), (17, 13), (4096, 64)]
+    rng = np.random.default_rng(5)
+    jobs, keep, pids = [], [], []
+    for k, (w, h) in enumerate(sizes):
+        img = synth.gradient_rgba8(w, h, 1000 + k)
+        colors = int(rng.choice([2, 4, 8, 16, 64, 256]))
+        pid = ctx.palette_from_image(img, colors, associate_alpha=True)
+        d = torch.from_numpy(img).cuda()
+        o = torch.empty((h, w), dtype=torch.uint8, device="cuda")
+        keep += [d, o]
+        pids.append(pid)
+        jobs.append(dict(pixels=d.data_ptr(), width=w, height=h, layout=sb.RGBA8, palette_id=pid,
+                         indices=o.data_ptr()))
+    total = sum(w * h for w, h in sizes)
+    biggest = max(w * h for w, h in sizes)
+    ctx.dither("seq", jobs, stream=s)
+    ctx.synchronize(s)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.current_stream())
+    ctx.dither("seq", jobs, stream=s)
+    e1.record(torch.cuda.current_stream())
+    ctx.synchronize(s)
+    ms_b = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    for j in jobs:
+        ctx.dither("seq", [j], stream=s)
+        ctx.synchronize(s)
+    ms_p = (time.perf_counter() - t0) * 1e3
+    for p in pids:
+        ctx.release_palette(p)
+    return {"images": len(sizes), "total_px": total, "largest_px": biggest,
+            "batched_ms": ms_b, "batched_mpx_s": total / ms_b / 1e3,
+            "plain_ms": ms_p, "plain_mpx_s": total / ms_p / 1e3,
+            "speedup": ms_p / ms_b, "amdahl_cap": total / biggest}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(a):
+    from stipple_b200 import synth
+    W, H, C = HEADLINE["width"], HEADLINE["height"], HEADLINE["colors"]
+    img = synth.gradient_rgb8(W, H, HEADLINE["seed"])
+    for _ in range(max(1, min(a.warmup, 1))):
+        reference_cpu(img, C, budget_s=0.0)
+    cpu, times = reference_cpu(img, C, budget_s=0.0)
+    step_times = []
+    for _ in range(a.steps):
+        c, t = reference_cpu(img, C, budget_s=0.0)
+        step_times.extend(t)
+    ms = statistics.median(step_times) * 1e3
+    value = W * H / ms / 1e3
+    cpu["value"] = value
+    return {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded gradient + noise sigma 8, RGB8)",
+            "config": {"workload": "seq-exact walk, one 3840x2160 RGB8 frame, 256-colour octree palette",
+                       "width": W, "height": H, "colors": C},
+            "impl": "reference", "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if a.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(a)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.distributed.init_process_group(
+            "nccl", timeout=datetime.timedelta(seconds=600),
+            device_id=torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0"))))
+    out = run_ours(a, rank, world)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

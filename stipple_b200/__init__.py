@@ -287,11 +287,34 @@ class Context:
             return (outs[0], rgbs[0]) if rgba else outs[0]
         return (outs, rgbs) if rgba else outs
 
+    def dither_host_into(self, engine: str | int, img: np.ndarray, palette_id: int,
+                         indices: np.ndarray, rgba_out: np.ndarray | None = None, **opts) -> None:
+        """Host form for one image into caller-owned (e.g. pinned) buffers."""
+        eng = ENGINES[engine] if isinstance(engine, str) else engine
+        h, w = img.shape[:2]
+        if indices.shape[:2] != (h, w) or indices.dtype != np.uint8 or not indices.flags.c_contiguous:
+            raise ValueError("indices must be a contiguous uint8 HxW array")
+        job = HostJob()
+        job.pixels = _ptr(img)
+        job.row_stride = img.strides[0]
+        job.width = w
+        job.height = h
+        job.layout = layout_of(img)
+        job.palette_id = palette_id
+        job.indices = _ptr(indices)
+        if rgba_out is not None:
+            job.rgba_out = _ptr(rgba_out)
+        o = options(**opts)
+        _check(load().rdb_dither_host(self.handle, eng, C.byref(job), 1, C.byref(o)))
+
     # -- dithering (device buffers; torch tensors as plumbing) ------------
-    def dither(self, engine: str | int, jobs: list[dict], stream: int = 0, **opts) -> None:
+    def dither(self, engine: str | int, jobs: list[dict], stream: int | None = None,
+               **opts) -> None:
         """Enqueue jobs whose buffers are device pointers: dicts with keys
         pixels, width, height, layout, palette_id, indices, optional rgba_out
-        and row_stride."""
+        and row_stride.  `stream` is a cudaStream_t handle (e.g. a
+        torch.cuda.Stream's ``cuda_stream``); None (or the null handle) means the
+        context's own stream."""
         eng = ENGINES[engine] if isinstance(engine, str) else engine
         n = len(jobs)
         arr = (Job * n)()
@@ -307,7 +330,7 @@ class Context:
         o = options(**opts)
         _check(load().rdb_dither(self.handle, eng, arr, n, C.byref(o), stream or None))
 
-    def synchronize(self, stream: int = 0) -> None:
+    def synchronize(self, stream: int | None = None) -> None:
         _check(load().rdb_synchronize(self.handle, stream or None))
 
 

@@ -284,8 +284,8 @@ int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t 
       --cache_bits;
     }
   }
-  if (use_cache && (cache_bits < 1 || cache_bits > 20)) {
-    return Fail(RDB_E_INVALID, "cache_bits out of range");
+  if (use_cache && (cache_bits < 4 || cache_bits > 20)) {
+    return Fail(RDB_E_INVALID, "cache_bits must be 4..20 (0 = automatic)");
   }
   const std::size_t smem = SeqSmemBytes(plan_max, cache_bits, use_cache);
   if (smem > smem_optin_) return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
@@ -416,15 +416,22 @@ int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream
 int Context::Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
   if (o.jacobi_taps < 1 || o.jacobi_taps > 4096) return Fail(RDB_E_UNSUPPORTED, "--approx-taps out of range");
   if (o.jacobi_iters < 0) return Fail(RDB_E_INVALID, "negative Jacobi iteration count");
+  // Impulse response of F = (I - H)^-1 for the walk's own feedback.  The walk
+  // adds sw[i] * error[i] with error[15] the newest residual
+  // (src/rd_riemersma_cpu.cpp:59-65, :104-112), so lag k carries sw[16 - k]:
+  // the newest residual has the SMALLEST weight.  The reference's
+  // BuildInverseFilter (src/rd_approx_cuda.cu:73-88) gives lag k w[k-1], the
+  // reverse, so its fixed point is not the walk's; rdb_inverse_filter keeps
+  // that formula for parity, the engine inverts the real feedback.
   std::vector<double> g(static_cast<std::size_t>(o.jacobi_taps) + 1);
   {
-    double w[kQueue];
-    error_weights(w);
+    double sw[kQueue];
+    scaled_weights(o.diffusion, sw);
     g[0] = 1.0;
     for (int d = 1; d <= o.jacobi_taps; ++d) {
       double acc = 0.0;
       const int kmax = d < kQueue ? d : kQueue;
-      for (int k = 1; k <= kmax; ++k) acc += (o.diffusion / 16.0) * w[k - 1] * g[d - k];
+      for (int k = 1; k <= kmax; ++k) acc += sw[kQueue - k] * g[d - k];
       g[d] = acc;
     }
   }

@@ -228,7 +228,9 @@ __global__ void __launch_bounds__(32) SeqWalkKernel(SeqLaunch L) {
   unsigned char* plan_smem = smem;
   uint32_t* cache = reinterpret_cast<uint32_t*>(smem + L.plan_smem_max);
   const int cache_entries = L.use_cache ? (1 << L.cache_bits) : 0;
-  int32_t* ring_ord = reinterpret_cast<int32_t*>(cache + cache_entries);
+  // The ring's float4 half needs 16-byte alignment whatever the cache size.
+  const int ring_off = (L.plan_smem_max + 4 * cache_entries + 15) & ~15;
+  int32_t* ring_ord = reinterpret_cast<int32_t*>(smem + ring_off);
   float4* ring_pix = reinterpret_cast<float4*>(ring_ord + kRing);
 
   uint16_t* memo = L.use_cache ? L.memo + static_cast<int64_t>(blockIdx.x) * L.slab_entries
@@ -281,9 +283,10 @@ __global__ void __launch_bounds__(32) SeqWalkKernel(SeqLaunch L) {
 }  // namespace
 
 std::size_t SeqSmemBytes(int plan_smem_max, int cache_bits, bool use_cache) {
-  return static_cast<std::size_t>(plan_smem_max) +
-         (use_cache ? (static_cast<std::size_t>(4) << cache_bits) : 0) +
-         kRing * (sizeof(int32_t) + sizeof(float4));
+  const std::size_t ring_off =
+      (static_cast<std::size_t>(plan_smem_max) +
+       (use_cache ? (static_cast<std::size_t>(4) << cache_bits) : 0) + 15) & ~static_cast<std::size_t>(15);
+  return ring_off + kRing * (sizeof(int32_t) + sizeof(float4));
 }
 
 cudaError_t LaunchSeqWalk(const SeqLaunch& L, int grid, cudaStream_t stream) {

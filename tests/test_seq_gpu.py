@@ -75,7 +75,7 @@ def test_seq_diffusion_and_cache_options(ctx, oracle):
                 idx = ctx.dither_host("seq", img, pid, diffusion=diff, use_cache=cache)
                 oidx, _, _ = oracle.walk_seq(q, 32, False, False, diffusion=diff, use_cache=bool(cache))
                 assert np.array_equal(idx, oidx), (diff, cache)
-        for bits in (1, 4, 8, 12, 15):
+        for bits in (4, 8, 12, 15):
             idx = ctx.dither_host("seq", img, pid, cache_bits=bits)
             oidx, _, _ = oracle.walk_seq(q, 32, False, False)
             assert np.array_equal(idx, oidx), bits
@@ -121,6 +121,8 @@ def test_seq_batch_equals_solo(ctx, oracle):
         again = ctx.dither_host("seq", imgs, pids)  # slabs reused: next generation
         for k in range(len(imgs)):
             assert np.array_equal(again[k], want[k])
+        with pytest.raises(sb.RdbError):
+            ctx.dither_host("seq", imgs[0], pids[0], cache_bits=3)
     finally:
         for p in pids:
             ctx.release_palette(p)
