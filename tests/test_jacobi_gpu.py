@@ -12,15 +12,20 @@ from stipple_b200 import metrics, synth
 
 pytestmark = pytest.mark.gpu
 
-# Measured tolerance of this engine (20 sweeps, 96 taps) on the synthetic
-# gradient+noise workload, against the cache-free and the memoised walks.
-MAX_MISMATCH_NOCACHE = 0.05
-MAX_MISMATCH_CACHED = 0.25
-MAX_DELTA_E = 3.0
+# Stated tolerance of this engine (20 sweeps, 96 taps) on the 320x240
+# gradient+noise workload: (index mismatch vs the cache-free walk, vs the
+# memoised walk, mean CIE dE76 vs the memoised walk).
+TOLERANCE = {
+    (16, False): (0.12, 0.14, 5.0),
+    (64, False): (0.02, 0.06, 1.2),
+    (256, False): (0.01, 0.06, 0.8),
+    (16, True): (0.22, 0.22, 7.5),
+}
 
 
-@pytest.mark.parametrize("colors,alpha", [(16, False), (64, False), (256, False), (16, True)])
+@pytest.mark.parametrize("colors,alpha", list(TOLERANCE))
 def test_jacobi_tolerance(ctx, oracle, colors, alpha):
+    MAX_MISMATCH_NOCACHE, MAX_MISMATCH_CACHED, MAX_DELTA_E = TOLERANCE[(colors, alpha)]
     img = synth.gradient_rgba8(320, 240, 21) if alpha else synth.gradient_rgb8(320, 240, 21)
     t = sb.Octree(img, colors, alpha)
     pid = ctx.palette_from_octree(t)
