@@ -167,6 +167,36 @@ typedef struct rdb_host_job {
 int rdb_dither_host(rdb_context* ctx, int engine, const rdb_host_job* jobs, int n_jobs,
                     const rdb_options* opts);
 
+/* Sequential-exact walk of one image without allocating any device memory.
+ * This entry point has no counterpart in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc: code running where a host
+ * framework owns every device allocation (a plugin inside an application with
+ * its own pooling allocator, which must not have memory taken behind its back),
+ * code on a latency-critical path where cudaMalloc's implicit device
+ * synchronisation is not acceptable, and code that must not fail halfway for
+ * lack of memory.  The caller passes the palette plan (host memory, made by
+ * rdb_plan_build), the pixels and the index map (device memory); everything
+ * else -- memo table, visit order, curve scratch, palette copy, launch
+ * descriptor -- lives in one fixed 5 MiB array in device memory that the
+ * library declares statically, so every GPU that loads the library holds it
+ * until the process exits.
+ *
+ * Limits: at most 4096 pixels per side and 1048576 pixels, palettes without
+ * associated alpha (an alpha memo has 2^24 keys), plan blob <= 64 KiB; larger
+ * inputs are refused with RDB_E_UNSUPPORTED and a message.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture on the device.  The work is
+ * enqueued on `stream` (NULL = legacy default stream); device-side status is
+ * not reported.  All calls share the one array and it keeps the last call's
+ * contents (the memo table is told apart by a generation counter, the work
+ * counter is cleared each call), so calls that overlap on the GPU -- on
+ * different streams, or from different threads -- race and corrupt each
+ * other's results: serialise them. */
+int rdb_dither_seq_noalloc(const void* plan, size_t plan_bytes, const void* pixels,
+                           size_t row_stride, int width, int height, int layout,
+                           uint8_t* indices, double diffusion, int use_cache, void* stream);
+
 /* Error weights 16^(-i/15) by ImageMagick's recurrence (rd_types.h:169-176)
  * and the Jacobi inverse filter (src/rd_approx_cuda.cu:73-88, exposed by the
  * reference as ApproxInverseFilter). */

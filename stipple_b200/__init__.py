@@ -105,6 +105,9 @@ SIGNATURES = {
     "rdb_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rdb_dither_host": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(HostJob), C.c_int,
                                   C.POINTER(Options)]),
+    "rdb_dither_seq_noalloc": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int,
+                                         C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_int,
+                                         C.c_void_p]),
     "rdb_error_weights": (None, [C.c_void_p]),
     "rdb_inverse_filter": (C.c_int, [C.c_int, C.c_double, C.c_void_p]),
     "rdb_block_gap": (C.c_int64, [C.c_int, C.c_int]),

@@ -73,12 +73,10 @@ RDB_HD unsigned cache_key(bool assoc, float r, float g, float b, float a) {
 }
 
 // rd_types.h:169-176 (the error weights 16^(-i/15), by IM's own recurrence).
-// Host only: std::exp/std::log.
-#if !defined(__CUDA_ARCH__)
+// Host functions (std::exp/std::log), defined in rdb_octree.cpp.
 void error_weights(double w[kQueue]);
 // scaled_w[k] = (kErrorRelativeWeight * diffusion) * weights[k],
 // src/rd_riemersma_cpu.cpp:370-373.
 void scaled_weights(double diffusion, double out[kQueue]);
-#endif
 
 }  // namespace rdb

@@ -29,7 +29,13 @@
 // lands on the chain.
 #include <cuda_runtime.h>
 
+#include <cstring>
+#include <mutex>
+
+#include "../../include/rdb.h"
+#include "rdb_curve.h"
 #include "rdb_device.cuh"
+#include "rdb_runtime.h"
 #include "rdb_walk.h"
 
 namespace rdb {
@@ -298,4 +304,144 @@ cudaError_t LaunchSeqWalk(const SeqLaunch& L, int grid, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------
+// The allocation-free sequential walk (rdb_dither_seq_noalloc in rdb.h).
+//
+// Everything the walk needs beyond the caller's pixels and index map -- the
+// memo table, the visit order, the curve-builder scratch, the palette plan
+// and the launch descriptor -- lives in one fixed array in device memory that
+// the library declares at file scope.  Every GPU that loads the library holds
+// it (a little over 5 MiB) until the process exits.  Host code never uses the
+// array's name as an address: the device address is fetched once per device
+// with cudaGetSymbolAddress.
+namespace noalloc {
+
+constexpr int kMaxSide = 4096;
+constexpr int64_t kMaxPixels = int64_t{1} << 20;
+constexpr std::size_t kMemoEntries = std::size_t{1} << 18;  // RGB keys: 6 bits per channel
+constexpr std::size_t kOffMemo = 0;
+constexpr std::size_t kOffMisc = kOffMemo + kMemoEntries * sizeof(uint16_t);  // 512 KiB
+constexpr std::size_t kOffItem = kOffMisc + 256;   // gen (4 B), counter (4 B), status (4 B)
+constexpr std::size_t kOffPlan = kOffItem + 256;
+constexpr std::size_t kPlanBytes = 64 * 1024;
+constexpr std::size_t kOffCurve = kOffPlan + kPlanBytes;
+constexpr std::size_t kCurveBytes = 512 * 1024;
+constexpr std::size_t kOffOrder = kOffCurve + kCurveBytes;
+constexpr std::size_t kBytes = kOffOrder + static_cast<std::size_t>(kMaxPixels) * sizeof(int32_t);
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_scratch[kBytes];
+
+std::mutex g_mu;
+unsigned char* g_base[kMaxDevices] = {};
+
+// Device address of g_scratch for the current device, looked up on the first
+// call made on that device.
+cudaError_t Base(int device, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_base[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+    if (e != cudaSuccess) return e;
+    g_base[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_base[device];
+  return cudaSuccess;
+}
+
+}  // namespace noalloc
+
 }  // namespace rdb
+
+extern "C" int rdb_dither_seq_noalloc(const void* plan, size_t plan_bytes, const void* pixels,
+                                      size_t row_stride, int width, int height, int layout,
+                                      uint8_t* indices, double diffusion, int use_cache,
+                                      void* stream) {
+  using namespace rdb;
+  namespace na = rdb::noalloc;
+  if (!plan || !pixels || !indices) return Fail(RDB_E_INVALID, "rdb_dither_seq_noalloc: null argument");
+  if (width < 1 || height < 1) return Fail(RDB_E_INVALID, "image must be at least 1x1");
+  if (width > na::kMaxSide || height > na::kMaxSide ||
+      static_cast<int64_t>(width) * height > na::kMaxPixels) {
+    return Fail(RDB_E_UNSUPPORTED,
+                "rdb_dither_seq_noalloc handles at most 4096 pixels per side and 1048576 pixels "
+                "(its scratch is a fixed 5 MiB device array); use rdb_dither for larger images");
+  }
+  if (layout != RDB_RGB8 && layout != RDB_RGBA8 && layout != RDB_RGBAF32) {
+    return Fail(RDB_E_INVALID, "unknown pixel layout");
+  }
+  const std::size_t bpp = layout == RDB_RGBAF32 ? 16 : static_cast<std::size_t>(layout);
+  const std::size_t stride = row_stride ? row_stride : static_cast<std::size_t>(width) * bpp;
+  if (stride < static_cast<std::size_t>(width) * bpp) return Fail(RDB_E_INVALID, "row stride shorter than a row");
+  if ((layout == RDB_RGBAF32 && ((reinterpret_cast<uintptr_t>(pixels) | stride) & 15u)) ||
+      (layout == RDB_RGBA8 && ((reinterpret_cast<uintptr_t>(pixels) | stride) & 3u))) {
+    return Fail(RDB_E_INVALID, "pixels or row stride misaligned for the layout");
+  }
+  if (plan_bytes < sizeof(PlanHeader)) return Fail(RDB_E_INVALID, "plan blob too short");
+  PlanHeader h;
+  std::memcpy(&h, plan, sizeof(h));
+  if (h.total_bytes != static_cast<int32_t>(plan_bytes) || h.smem_bytes <= 0 ||
+      h.smem_bytes > h.total_bytes || h.count < 1 || h.count > kMaxPaletteColors) {
+    return Fail(RDB_E_INVALID, "not a plan blob from rdb_plan_build");
+  }
+  if (h.assoc) {
+    return Fail(RDB_E_UNSUPPORTED,
+                "rdb_dither_seq_noalloc takes palettes without associated alpha only (an alpha "
+                "memo table has 2^24 keys and does not fit the fixed scratch)");
+  }
+  if (plan_bytes > na::kPlanBytes) return Fail(RDB_E_UNSUPPORTED, "palette plan larger than 64 KiB");
+  const int level = CurveLevel(width, height);
+  if (CurveScratchBytes(level) > na::kCurveBytes) return Fail(RDB_E_UNSUPPORTED, "curve scratch too small");
+
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return CudaFail(e, "cudaGetDevice");
+  if (device < 0 || device >= na::kMaxDevices) return Fail(RDB_E_UNSUPPORTED, "device index too large");
+  unsigned char* base = nullptr;
+  if ((e = na::Base(device, &base)) != cudaSuccess) return CudaFail(e, "cudaGetSymbolAddress");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  uint32_t* misc = reinterpret_cast<uint32_t*>(base + na::kOffMisc);  // [0] gen, [1] counter, [2] status
+  int32_t* order = reinterpret_cast<int32_t*>(base + na::kOffOrder);
+  unsigned char* dplan = base + na::kOffPlan;
+  SeqItem item{};
+  item.pixels = static_cast<const unsigned char*>(pixels);
+  item.row_stride = static_cast<int64_t>(stride);
+  item.width = width;
+  item.height = height;
+  item.layout = layout;
+  item.n = width * height;
+  item.order = order;
+  item.indices = indices;
+  item.rgba_out = nullptr;
+  item.plan = dplan;
+  item.plan_smem = h.smem_bytes;
+  // The counter and status start at zero on every call; the memo slab keeps
+  // its contents and is told apart by the generation in misc[0].
+  if ((e = cudaMemsetAsync(misc + 1, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dplan, plan, plan_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(base + na::kOffItem, &item, sizeof(item), cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess) {
+    return CudaFail(e, "rdb_dither_seq_noalloc staging");
+  }
+  if ((e = BuildSeqOrder(width, height, order, base + na::kOffCurve, na::kCurveBytes, s)) != cudaSuccess) {
+    return CudaFail(e, "visit order kernel");
+  }
+  SeqLaunch L{};
+  L.items = reinterpret_cast<const SeqItem*>(base + na::kOffItem);
+  L.n_items = 1;
+  L.work_counter = reinterpret_cast<int*>(misc + 1);
+  L.memo = reinterpret_cast<uint16_t*>(base + na::kOffMemo);
+  L.memo_gen = misc;
+  L.slab_entries = static_cast<int64_t>(na::kMemoEntries);
+  L.use_cache = use_cache ? 1 : 0;
+  L.cache_bits = use_cache ? 15 : 0;
+  L.plan_smem_max = h.smem_bytes;
+  while (use_cache && L.cache_bits > 8 && SeqSmemBytes(L.plan_smem_max, L.cache_bits, true) > 227 * 1024) {
+    --L.cache_bits;
+  }
+  scaled_weights(diffusion, L.sw);
+  L.status = reinterpret_cast<int*>(misc + 2);
+  if ((e = LaunchSeqWalk(L, 1, s)) != cudaSuccess) return CudaFail(e, "sequential walk launch");
+  return RDB_OK;
+}
