@@ -117,6 +117,12 @@ std::string BuildPlan(const PlanInput& in, std::vector<uint8_t>* blob) {
   off = Align16(off + static_cast<std::size_t>(nodes) * 2 * sizeof(uint16_t));
   h.off_seq = static_cast<int32_t>(off);
   off = Align16(off + static_cast<std::size_t>(slots > 0 ? slots : 1));
+  h.slot_stride = (slots + 1) & ~1;
+  h.off_slotpal = static_cast<int32_t>(off);
+  off = Align16(off + static_cast<std::size_t>(4) * h.slot_stride * sizeof(double));
+  const int jump_entries = 1 << (kJumpLevels * (in.assoc ? 4 : 3));
+  h.off_jump = static_cast<int32_t>(off);
+  off = Align16(off + static_cast<std::size_t>(jump_entries) * sizeof(uint16_t));
   h.smem_bytes = static_cast<int32_t>(off);
   h.off_out = static_cast<int32_t>(off);
   off = Align16(off + static_cast<std::size_t>(in.count) * 4 * sizeof(float));
@@ -180,6 +186,39 @@ std::string BuildPlan(const PlanInput& in, std::vector<uint8_t>* blob) {
     range[2 * l + 1] = static_cast<uint16_t>(span[p]);
   }
   std::memcpy(b + h.off_seq, seq.data(), seq.size());
+
+  // Distance-side colours in slot order, one row per channel, so a search
+  // over a run of slots reads consecutive doubles.
+  double* slotpal = reinterpret_cast<double*>(b + h.off_slotpal);
+  for (int s = 0; s < slots; ++s) {
+    const double* e = reinterpret_cast<const double*>(b + h.off_pal +
+                                                      static_cast<std::size_t>(seq[s]) * pal_stride);
+    for (int c = 0; c < 4; ++c) slotpal[static_cast<std::size_t>(c) * h.slot_stride + s] = e[c];
+  }
+
+  // The first kJumpLevels levels of the descent (src/rd_riemersma_cpu.cpp:84-89)
+  // for every combination of the top bits.
+  uint16_t* jump = reinterpret_cast<uint16_t*>(b + h.off_jump);
+  const int bits = in.assoc ? 4 : 3;
+  for (int idx = 0; idx < jump_entries; ++idx) {
+    int node = 0;
+    bool stopped = false;
+    for (int level = 0; level < kJumpLevels && !stopped; ++level) {
+      const int bit = kJumpLevels - 1 - level;  // top bit first
+      int id = 0;
+      for (int c = 0; c < bits; ++c) {
+        const int top = (idx >> (kJumpLevels * c)) & ((1 << kJumpLevels) - 1);
+        id |= ((top >> bit) & 1) << c;
+      }
+      const int16_t next = child[node * fan + id];
+      if (next < 0) {
+        stopped = true;
+      } else {
+        node = next;
+      }
+    }
+    jump[idx] = static_cast<uint16_t>(node | (stopped ? 0x8000 : 0));
+  }
   return std::string();
 }
 

@@ -48,8 +48,15 @@ struct PlanHeader {
   int32_t off_seq;
   int32_t off_out;
   int32_t pal_stride; // bytes per PalEntry: 32 (no alpha) or 64 (alpha)
-  int32_t pad[3];
+  int32_t off_slotpal;  // channel-planar distance-side colours in slot order: 4 x slot_stride doubles
+  int32_t off_jump;     // descent after the first kJumpLevels levels, indexed by the top bits
+  int32_t slot_stride;  // doubles per channel row of slotpal (slots rounded up to even)
 };
+// The first three levels of the descent collapse into one table lookup: the
+// index is the top three bits of each channel's byte (r | g << 3 | b << 6 |
+// a << 9), the entry the live node reached (bit 15 set when the descent had
+// already stopped at a missing child within those levels).
+constexpr int kJumpLevels = 3;
 static_assert(sizeof(PlanHeader) == 64, "header is one 64-byte block");
 
 // Without alpha the distance-side and residual-side colours coincide, so an

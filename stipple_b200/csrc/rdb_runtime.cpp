@@ -406,6 +406,8 @@ int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream
   L.cx_offset = static_cast<int64_t*>(block_offsets_.ptr);
   L.plan = p->dev;
   L.plan_smem = p->smem;
+  L.assoc = p->assoc ? 1 : 0;
+  L.is_float = layout == RDB_RGBAF32 ? 1 : 0;
   scaled_weights(o.diffusion, L.sw);
   L.status = static_cast<int*>(status_.ptr);
   e = LaunchBlockWalk(L, positions, s);

@@ -70,6 +70,8 @@ struct BlockLaunch {
   int64_t* cx_offset;           // per image: offset of its curve positions in cx/chosen
   const unsigned char* plan;    // one palette for the launch
   int plan_smem;
+  int assoc;                    // the palette associates alpha
+  int is_float;                 // RgbaF input (cx holds float4 per position)
   int pad;
   double sw[16];
   int* status;

@@ -22,6 +22,7 @@
 #include "rdb_curve.h"
 #include "rdb_device.cuh"
 #include "rdb_walk.h"
+#include "rdb_walk_thread.cuh"
 
 namespace rdb {
 namespace {
@@ -76,80 +77,139 @@ __global__ void BlockGather(BlockLaunch L, int64_t total) {
   }
 }
 
-__device__ __forceinline__ V4 unpack(int assoc, uint32_t w) {
-  float4 s = make_float4(static_cast<float>(w & 0xFFu) * 257.0f,
-                         static_cast<float>((w >> 8) & 0xFFu) * 257.0f,
-                         static_cast<float>((w >> 16) & 0xFFu) * 257.0f,
-                         static_cast<float>(w >> 24) * 257.0f);
-  V4 v;
-  associate_sample(assoc, s, v.r, v.g, v.b, v.a);
-  return v;
-}
-
-template <bool kAssoc, bool kFloat>
-__device__ __forceinline__ V4 sample_at(const BlockLaunch& L, int64_t i) {
-  if (kFloat) {
-    V4 v;
-    associate_sample(kAssoc, reinterpret_cast<const float4*>(L.cx)[i], v.r, v.g, v.b, v.a);
-    return v;
-  }
-  return unpack(kAssoc, L.cx[i]);
-}
-
-template <bool kAssoc, bool kFloat>
-__device__ void WalkBlock(const BlockLaunch& L, const PlanView& P, int64_t base, int begin,
-                          int end) {
-  double sw[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) sw[k] = L.sw[k];
-  V4 R[16];
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    R[j] = (begin + j < end) ? sample_at<kAssoc, kFloat>(L, base + begin + j)
-                             : V4{0.0, 0.0, 0.0, 0.0};
-  }
-  V4 e{0.0, 0.0, 0.0, 0.0};
-  for (int g0 = begin; g0 < end; g0 += 16) {
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int t = g0 + u;
-      if (t < end) {
-        V4 v;
-        v.r = __dadd_rn(R[u].r, __dmul_rn(sw[15], e.r));
-        v.g = __dadd_rn(R[u].g, __dmul_rn(sw[15], e.g));
-        v.b = __dadd_rn(R[u].b, __dmul_rn(sw[15], e.b));
-        if (kAssoc) v.a = __dadd_rn(R[u].a, __dmul_rn(sw[15], e.a));
-#pragma unroll
-        for (int j = 1; j < 16; ++j) {
-          V4& s = R[(u + j) & 15];
-          s.r = __dadd_rn(s.r, __dmul_rn(sw[15 - j], e.r));
-          s.g = __dadd_rn(s.g, __dmul_rn(sw[15 - j], e.g));
-          s.b = __dadd_rn(s.b, __dmul_rn(sw[15 - j], e.b));
-          if (kAssoc) s.a = __dadd_rn(s.a, __dmul_rn(sw[15 - j], e.a));
-        }
-        R[u] = (t + 16 < end) ? sample_at<kAssoc, kFloat>(L, base + t + 16)
-                              : V4{0.0, 0.0, 0.0, 0.0};
-        const float fr = clamp_pixel(v.r);
-        const float fg = clamp_pixel(v.g);
-        const float fb = clamp_pixel(v.b);
-        const float fa = kAssoc ? clamp_pixel(v.a) : 0.0f;
-        const int node = plan_descend(P, byte_dev(fr), byte_dev(fg), byte_dev(fb),
-                                      kAssoc ? byte_dev(fa) : 0u);
-        const Target tg = make_target(kAssoc, static_cast<double>(fr), static_cast<double>(fg),
-                                      static_cast<double>(fb), static_cast<double>(fa));
-        const int index = plan_search_serial(P, node, tg);
-        L.chosen[base + t] = static_cast<uint8_t>(index);
-        const double* rc = P.rcol(index);
-        e.r = __dadd_rn(static_cast<double>(fr), -rc[0]);
-        e.g = __dadd_rn(static_cast<double>(fg), -rc[1]);
-        e.b = __dadd_rn(static_cast<double>(fb), -rc[2]);
-        if (kAssoc) e.a = __dadd_rn(static_cast<double>(fa), -rc[3]);
-      }
+// Channel c of AssociateAlphaPixel (rd_types.h:179-192) for a packed RGBA8
+// sample: the Q16 value is v * 257, exact in double.
+template <bool kAssoc>
+__device__ __forceinline__ void unpack8(uint32_t w, double (&p)[4]) {
+  const double r = static_cast<double>((w & 0xFFu) * 257u);
+  const double g = static_cast<double>(((w >> 8) & 0xFFu) * 257u);
+  const double b = static_cast<double>(((w >> 16) & 0xFFu) * 257u);
+  const unsigned a8 = w >> 24;
+  p[0] = r;
+  p[1] = g;
+  p[2] = b;
+  if (kAssoc) {
+    const double a = static_cast<double>(a8 * 257u);
+    p[3] = a;
+    if (a8 != 255u) {
+      const double alpha = __dmul_rn(kQuantumScale, a);
+      p[0] = __dmul_rn(alpha, r);
+      p[1] = __dmul_rn(alpha, g);
+      p[2] = __dmul_rn(alpha, b);
     }
   }
 }
 
-__global__ void __launch_bounds__(128) BlockWalkKernel(BlockLaunch L) {
+template <bool kAssoc>
+__device__ __forceinline__ void unpackf(float4 s, double (&p)[4]) {
+  associate_sample(kAssoc, s, p[0], p[1], p[2], p[3]);
+}
+
+// One step of the running sums with the rotation fixed at compile time:
+// pixel t (slot U) takes its last term, the 15 pixels after it take theirs,
+// and slot U is refilled with pixel t+16.
+template <int U, int C>
+__device__ __forceinline__ void RotateSums(const BlockLaunch& L, double (&R)[16][C],
+                                           const double (&e)[C], double (&v)[C],
+                                           const double (&p)[4]) {
+#pragma unroll
+  for (int k = 0; k < C; ++k) v[k] = __dadd_rn(R[U][k], __dmul_rn(L.sw[15], e[k]));
+#pragma unroll
+  for (int jj = 1; jj < 16; ++jj) {
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+      R[(U + jj) & 15][k] = __dadd_rn(R[(U + jj) & 15][k], __dmul_rn(L.sw[15 - jj], e[k]));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < C; ++k) R[U][k] = p[k];
+}
+
+// One block: positions [begin, end) of one image's list, zeroed queue, no
+// memo.  Only the register rotation is unrolled (16 switch cases of FP64
+// work); the lookup is written once, so the loop stays in the instruction
+// cache.
+template <bool kAssoc, bool kFloat>
+__device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& P, int64_t base,
+                                          int begin, int end) {
+  constexpr int C = kAssoc ? 4 : 3;
+  const uint32_t* cx = L.cx + base;
+  const float4* cxf = reinterpret_cast<const float4*>(L.cx) + base;
+  double R[16][C];
+  double e[C];
+#pragma unroll
+  for (int k = 0; k < C; ++k) e[k] = 0.0;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
+    if (begin + u < end) {
+      if (kFloat) unpackf<kAssoc>(cxf[begin + u], p); else unpack8<kAssoc>(cx[begin + u], p);
+    }
+#pragma unroll
+    for (int k = 0; k < C; ++k) R[u][k] = p[k];
+  }
+  const bool word_out = ((base + begin) & 3) == 0;
+  uint32_t acc = 0;
+  int u = 0;
+#pragma unroll 1
+  for (int t = begin; t < end; ++t) {
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
+    if (t + 16 < end) {
+      if (kFloat) unpackf<kAssoc>(cxf[t + 16], p); else unpack8<kAssoc>(cx[t + 16], p);
+    }
+    double v[C];
+    switch (u) {
+      case 0: RotateSums<0, C>(L, R, e, v, p); break;
+      case 1: RotateSums<1, C>(L, R, e, v, p); break;
+      case 2: RotateSums<2, C>(L, R, e, v, p); break;
+      case 3: RotateSums<3, C>(L, R, e, v, p); break;
+      case 4: RotateSums<4, C>(L, R, e, v, p); break;
+      case 5: RotateSums<5, C>(L, R, e, v, p); break;
+      case 6: RotateSums<6, C>(L, R, e, v, p); break;
+      case 7: RotateSums<7, C>(L, R, e, v, p); break;
+      case 8: RotateSums<8, C>(L, R, e, v, p); break;
+      case 9: RotateSums<9, C>(L, R, e, v, p); break;
+      case 10: RotateSums<10, C>(L, R, e, v, p); break;
+      case 11: RotateSums<11, C>(L, R, e, v, p); break;
+      case 12: RotateSums<12, C>(L, R, e, v, p); break;
+      case 13: RotateSums<13, C>(L, R, e, v, p); break;
+      case 14: RotateSums<14, C>(L, R, e, v, p); break;
+      default: RotateSums<15, C>(L, R, e, v, p); break;
+    }
+    u = (u + 1) & 15;
+    float f[4];
+#pragma unroll
+    for (int k = 0; k < C; ++k) f[k] = clamp_pixel(v[k]);
+    const unsigned ba = kAssoc ? byte_dev(f[C - 1]) : 0u;
+    const int node = tw::descend<kAssoc>(P, byte_dev(f[0]), byte_dev(f[1]), byte_dev(f[2]), ba);
+    double tr = f[0], tg = f[1], tb = f[2], ta = 0.0;
+    if (kAssoc) {
+      ta = f[3];
+      const double beta = __dmul_rn(kQuantumScale, ta);
+      tr = __dmul_rn(beta, tr);
+      tg = __dmul_rn(beta, tg);
+      tb = __dmul_rn(beta, tb);
+    }
+    const int index = tw::search<kAssoc>(P, node, tr, tg, tb, ta);
+    const double* rc = P.rcol<kAssoc>(index);
+#pragma unroll
+    for (int k = 0; k < C; ++k) e[k] = __dadd_rn(static_cast<double>(f[k]), -rc[k]);
+    if (word_out) {
+      const int q = (t - begin) & 3;
+      acc |= static_cast<uint32_t>(index) << (8 * q);
+      if (q == 3) {
+        *reinterpret_cast<uint32_t*>(L.chosen + base + t - 3) = acc;
+        acc = 0;
+      } else if (t == end - 1) {
+        for (int r = 0; r <= q; ++r) L.chosen[base + t - q + r] = static_cast<uint8_t>(acc >> (8 * r));
+      }
+    } else {
+      L.chosen[base + t] = static_cast<uint8_t>(index);
+    }
+  }
+}
+template <bool kAssoc, bool kFloat>
+__global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   {
     const int4* src = reinterpret_cast<const int4*>(L.plan);
@@ -159,24 +219,25 @@ __global__ void __launch_bounds__(128) BlockWalkKernel(BlockLaunch L) {
   __syncthreads();
   const int64_t gb = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (gb >= L.total_blocks) return;
-  PlanView P;
+  tw::Plan P;
   P.bind(smem);
   const int im = find_image(L.images, L.n_images, gb);
   const BlockImage& I = L.images[im];
   const int b = static_cast<int>(gb - I.first_block);
   const int begin = b * L.block;
   const int end = min(begin + L.block, I.n);
-  const int64_t base = L.cx_offset[im];
-  const bool is_float = I.layout == 16;
-  if (P.assoc) {
-    if (is_float) WalkBlock<true, true>(L, P, base, begin, end);
-    else WalkBlock<true, false>(L, P, base, begin, end);
-  } else {
-    if (is_float) WalkBlock<false, true>(L, P, base, begin, end);
-    else WalkBlock<false, false>(L, P, base, begin, end);
-  }
+  WalkBlock<kAssoc, kFloat>(L, P, L.cx_offset[im], begin, end);
 }
 
+template <bool kAssoc, bool kFloat>
+cudaError_t LaunchWalk(const BlockLaunch& L, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(BlockWalkKernel<kAssoc, kFloat>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L.plan_smem);
+  if (e != cudaSuccess) return e;
+  const unsigned g2 = static_cast<unsigned>((L.total_blocks + 127) / 128);
+  BlockWalkKernel<kAssoc, kFloat><<<g2, 128, L.plan_smem, stream>>>(L);
+  return cudaGetLastError();
+}
 // Owner-map scatter (src/rd_riemersma_cpu.cpp:698-710): position 0 is the
 // origin's first visit and the final position its last, so every position
 // but 0 owns its pixel.  The unvisited cell, if any, is copied from the
@@ -237,11 +298,11 @@ cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaS
   if (total_positions <= 0 || L.total_blocks <= 0) return cudaSuccess;
   const unsigned g1 = static_cast<unsigned>((total_positions + 255) / 256);
   BlockGather<<<g1, 256, 0, stream>>>(L, total_positions);
-  cudaError_t e = cudaFuncSetAttribute(BlockWalkKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       L.plan_smem);
+  const PlanHeader* hp = nullptr;
+  (void)hp;
+  cudaError_t e = L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, stream) : LaunchWalk<true, false>(L, stream))
+                          : (L.is_float ? LaunchWalk<false, true>(L, stream) : LaunchWalk<false, false>(L, stream));
   if (e != cudaSuccess) return e;
-  const unsigned g2 = static_cast<unsigned>((L.total_blocks + 127) / 128);
-  BlockWalkKernel<<<g2, 128, L.plan_smem, stream>>>(L);
   BlockScatter<<<g1, 256, 0, stream>>>(L, total_positions);
   return cudaGetLastError();
 }

@@ -79,6 +79,9 @@ def test_seq_diffusion_and_cache_options(ctx, oracle):
             idx = ctx.dither_host("seq", img, pid, cache_bits=bits)
             oidx, _, _ = oracle.walk_seq(q, 32, False, False)
             assert np.array_equal(idx, oidx), bits
+        # 2^17 entries do not fit in shared memory: refused, not truncated.
+        with pytest.raises(sb.RdbError):
+            ctx.dither_host("seq", img, pid, cache_bits=17)
     finally:
         ctx.release_palette(pid)
 
