@@ -130,7 +130,13 @@ typedef struct rdb_options {
   int jacobi_taps;      /* default 96 (ApproxOptions::taps), 1..4096 */
   int jacobi_fp64;      /* default 0 (ApproxOptions::fp64) */
   int cache_bits;       /* sequential engine: log2 shared-memory memo cache entries, 0 = auto */
-  int reserved[8];
+  int seq_mode;         /* sequential engine: 0 = auto, 1 = one warp walks each image whole,
+                           2 = speculative segmented walk (exact; see rdb_ssw.h) */
+  int seg_len;          /* segmented walk: positions per segment, 0 = auto */
+  int warm_len;         /* segmented walk: warm-up positions before each segment, 0 = auto */
+  int max_passes;       /* segmented walk: give up after this many passes (0 = no limit); the
+                           walk then reports RDB_E_DEVICE -- never an inexact result */
+  int reserved[4];
 } rdb_options;
 
 void rdb_options_default(rdb_options* o);

@@ -40,7 +40,11 @@ class Options(C.Structure):
         ("jacobi_taps", C.c_int),
         ("jacobi_fp64", C.c_int),
         ("cache_bits", C.c_int),
-        ("reserved", C.c_int * 8),
+        ("seq_mode", C.c_int),
+        ("seg_len", C.c_int),
+        ("warm_len", C.c_int),
+        ("max_passes", C.c_int),
+        ("reserved", C.c_int * 4),
     ]
 
 

@@ -40,6 +40,7 @@ SOURCES = [
     "rdb_walk_seq.cu",
     "rdb_walk_blocks.cu",
     "rdb_jacobi.cu",
+    "rdb_ssw.cu",
 ]
 
 

@@ -236,6 +236,10 @@ void rdb_options_default(rdb_options* o) {
   o->jacobi_taps = 96;
   o->jacobi_fp64 = 0;
   o->cache_bits = 0;
+  o->seq_mode = 0;
+  o->seg_len = 0;
+  o->warm_len = 0;
+  o->max_passes = 0;
 }
 
 int rdb_dither(rdb_context* ctx, int engine, const rdb_job* jobs, int n_jobs,

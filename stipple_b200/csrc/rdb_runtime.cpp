@@ -7,6 +7,7 @@
 
 #include "rdb_curve.h"
 #include "rdb_numeric.h"
+#include "rdb_ssw.h"
 
 namespace rdb {
 namespace {
@@ -43,7 +44,8 @@ Context::~Context() {
   for (auto& o : orders_) cudaFree(o.second);
   for (DevBuf* b : {&memo_, &memo_gen_, &seq_items_, &counter_, &status_, &curve_scratch_,
                     &block_images_, &block_offsets_, &block_cx_, &block_chosen_, &jac_cx_,
-                    &jac_q_, &jac_g_, &host_in_, &host_idx_, &host_rgba_}) {
+                    &jac_q_, &jac_g_, &host_in_, &host_idx_, &host_rgba_, &ssw_images_,
+                    &ssw_segs_, &ssw_work_, &ssw_q_, &ssw_ltab_, &ssw_g_, &ssw_bad_}) {
     Release(b);
   }
   if (stream_) cudaStreamDestroy(stream_);
@@ -233,7 +235,14 @@ int Context::Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o
   if (!s) s = stream_;
   cudaSetDevice(device_);
   switch (engine) {
-    case RDB_ENGINE_SEQ: return Seq(jobs, n, o, s);
+    case RDB_ENGINE_SEQ: {
+      if (o.seq_mode == 1) return Seq(jobs, n, o, s);
+      if (o.seq_mode == 2) return SeqSegmented(jobs, n, o, s);
+      // Automatic: segment once any image is long enough to split.
+      int64_t longest = 0;
+      for (int i = 0; i < n; ++i) longest = std::max<int64_t>(longest, int64_t{jobs[i].width} * jobs[i].height);
+      return longest >= 8192 ? SeqSegmented(jobs, n, o, s) : Seq(jobs, n, o, s);
+    }
     case RDB_ENGINE_BLOCKS: return Blocks(jobs, n, o, s);
     case RDB_ENGINE_JACOBI: return Jacobi(jobs, n, o, s);
     default: return Fail(RDB_E_INVALID, "unknown engine");
@@ -567,6 +576,196 @@ int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_o
     }
   }
   return Synchronize(s);
+}
+
+// The speculative segmented walk (rdb_ssw.h): every image is cut into
+// segments, all segments of all images run as one persistent launch per pass,
+// and passes repeat until each image's verified prefix covers it.
+int Context::SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  const bool use_cache = o.use_cache != 0;
+  const int seg_len = o.seg_len > 0 ? std::max(o.seg_len, 64) : 2048;
+  const int warm_len = o.warm_len > 0 ? o.warm_len : 1024;
+  std::vector<SswImage> imgs(static_cast<std::size_t>(n));
+  std::vector<SswSeg> segs;
+  int plan_max = 0;
+  bool any_assoc = false;
+  std::size_t g_bytes = 0;
+  std::vector<std::size_t> g_off(static_cast<std::size_t>(n));
+  std::vector<uint32_t> g_cap(static_cast<std::size_t>(n));
+  int max_seg = 0;
+  for (int i = 0; i < n; ++i) {
+    const rdb_job& j = jobs[i];
+    const DevPlan* p = Plan(j.palette_id);
+    const int32_t* order = nullptr;
+    if (int rc = Order(j.width, j.height, s, &order)) return rc;
+    SswImage& im = imgs[static_cast<std::size_t>(i)];
+    std::memset(&im, 0, sizeof(im));
+    im.pixels = static_cast<const unsigned char*>(j.pixels);
+    im.row_stride = static_cast<int64_t>(RowStride(j));
+    im.width = j.width;
+    im.height = j.height;
+    im.layout = j.layout;
+    im.n = j.width * j.height;
+    im.order = order;
+    im.indices = j.indices;
+    im.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+    im.plan = p->dev;
+    im.plan_smem = p->smem;
+    im.assoc = p->assoc ? 1 : 0;
+    plan_max = std::max(plan_max, p->smem);
+    any_assoc = any_assoc || p->assoc;
+    // Segments of [seg_len, 2 seg_len) positions; a short image is one segment.
+    const int k_count = std::max(1, im.n / seg_len);
+    im.first_seg = static_cast<int>(segs.size());
+    im.nsegs = k_count;
+    for (int k = 0; k < k_count; ++k) {
+      SswSeg sg{};
+      sg.image = i;
+      sg.k = k;
+      sg.begin = k * seg_len;
+      sg.end = (k == k_count - 1) ? im.n : (k + 1) * seg_len;
+      sg.warm = k == 0 ? 0 : std::min(sg.begin, warm_len);
+      sg.run_tag = 0;
+      max_seg = std::max(max_seg, sg.end - sg.begin);
+      segs.push_back(sg);
+    }
+    // G: a direct 2^18 table for RGB keys, a hash sized for the image otherwise.
+    uint32_t cap = 1u << 18;
+    if (p->assoc) {
+      cap = 1024;
+      const int64_t want = std::min<int64_t>(2 * static_cast<int64_t>(im.n), int64_t{1} << 25);
+      while (static_cast<int64_t>(cap) < want) cap <<= 1;
+    }
+    g_cap[i] = cap;
+    g_off[i] = g_bytes;
+    g_bytes += static_cast<std::size_t>(cap) * (p->assoc ? 16 : 8);  // 2 buffers x (vals [+ keys])
+  }
+  const int total = static_cast<int>(segs.size());
+  // L tables: room for twice the distinct keys a segment can touch.
+  int ltab_bits = 6;
+  const int64_t key_space = any_assoc ? (int64_t{1} << 24) : (int64_t{1} << 18);
+  while ((int64_t{1} << ltab_bits) < std::min<int64_t>(2 * static_cast<int64_t>(max_seg), 2 * key_space)) {
+    ++ltab_bits;
+  }
+  const std::size_t ltab_bytes = static_cast<std::size_t>(total) << (ltab_bits + 3);
+  const std::size_t q_bytes = static_cast<std::size_t>(total) * 64 * sizeof(double);
+  if (int rc = Reserve(&ssw_images_, imgs.size() * sizeof(SswImage), "segmented walk images")) return rc;
+  if (int rc = Reserve(&ssw_segs_, segs.size() * sizeof(SswSeg), "segments")) return rc;
+  if (int rc = Reserve(&ssw_work_, segs.size() * sizeof(int), "segment work list")) return rc;
+  if (int rc = Reserve(&ssw_q_, 2 * q_bytes, "segment queues")) return rc;
+  if (use_cache && Reserve(&ssw_ltab_, ltab_bytes, "segment memo tables")) return RDB_E_NOMEM;
+  if (use_cache && Reserve(&ssw_g_, g_bytes, "first-touch maps")) return RDB_E_NOMEM;
+  if (int rc = Reserve(&ssw_bad_, imgs.size() * sizeof(int), "verification flags")) return rc;
+  unsigned char* gbase = static_cast<unsigned char*>(ssw_g_.ptr);
+  for (int i = 0; i < n; ++i) {
+    SswImage& im = imgs[static_cast<std::size_t>(i)];
+    if (!use_cache) continue;
+    const uint32_t cap = g_cap[i];
+    uint32_t* base = reinterpret_cast<uint32_t*>(gbase + g_off[i]);
+    im.g_vals[0] = base;
+    im.g_vals[1] = base + cap;
+    if (im.assoc) {
+      im.g_keys[0] = base + 2 * static_cast<std::size_t>(cap);
+      im.g_keys[1] = base + 3 * static_cast<std::size_t>(cap);
+      im.g_mask = cap - 1;
+    }
+  }
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(ssw_images_.ptr, imgs.data(), imgs.size() * sizeof(SswImage),
+                           cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ssw_segs_.ptr, segs.data(), segs.size() * sizeof(SswSeg),
+                           cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+    return CudaFail(e, "segment upload");
+  }
+  double* q_start = static_cast<double*>(ssw_q_.ptr);
+  double* q_end = q_start + static_cast<std::size_t>(total) * 64;
+  cudaMemsetAsync(q_start, 0, 2 * q_bytes, s);
+  if (use_cache) {
+    cudaMemsetAsync(ssw_ltab_.ptr, 0, ltab_bytes, s);
+    // G buffer 0 (read by pass 0) empty: vals all ones, keys zero.
+    for (int i = 0; i < n; ++i) {
+      const SswImage& im = imgs[static_cast<std::size_t>(i)];
+      cudaMemsetAsync(im.g_vals[0], 0xFF, static_cast<std::size_t>(g_cap[i]) * 4, s);
+      if (im.assoc) cudaMemsetAsync(im.g_keys[0], 0, static_cast<std::size_t>(g_cap[i]) * 4, s);
+    }
+  }
+
+  // Shared memory per warp: the largest plan, a memo cache, the pixel ring.
+  int cache_bits = o.cache_bits > 0 ? o.cache_bits : 11;
+  if (cache_bits < 4 || cache_bits > 20) return Fail(RDB_E_INVALID, "cache_bits must be 4..20 (0 = automatic)");
+  const std::size_t smem = SswSmemBytes(plan_max, cache_bits);
+  if (smem > smem_optin_) return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
+  const int per_sm = std::max(1, std::min<int>(16, static_cast<int>((228 * 1024) / (smem + 1024))));
+
+  SswLaunch L{};
+  L.images = static_cast<const SswImage*>(ssw_images_.ptr);
+  L.segs = static_cast<SswSeg*>(ssw_segs_.ptr);
+  L.work = static_cast<const int*>(ssw_work_.ptr);
+  L.q_start = q_start;
+  L.q_end = q_end;
+  L.ltab = static_cast<uint64_t*>(ssw_ltab_.ptr);
+  L.ltab_bits = ltab_bits;
+  L.use_cache = use_cache ? 1 : 0;
+  L.cache_bits = cache_bits;
+  L.plan_smem_max = plan_max;
+  L.counter = static_cast<int*>(counter_.ptr);
+  L.first_bad = static_cast<int*>(ssw_bad_.ptr);
+  L.status = static_cast<int*>(status_.ptr);
+  scaled_weights(o.diffusion, L.sw);
+
+  std::vector<int> verified(static_cast<std::size_t>(n), 0);
+  std::vector<int> bad(static_cast<std::size_t>(n));
+  std::vector<int> work;
+  const int max_passes = o.max_passes > 0 ? o.max_passes : 1 << 30;
+  int pass = 0;
+  for (;; ++pass) {
+    if (pass >= max_passes || pass >= 255) {
+      return Fail(RDB_E_DEVICE, "segmented walk did not converge within the pass limit");
+    }
+    work.clear();
+    for (int i = 0; i < n; ++i) {
+      for (int k = verified[i]; k < imgs[i].nsegs; ++k) work.push_back(imgs[i].first_seg + k);
+    }
+    if (work.empty()) break;
+    L.pass = pass;
+    L.tag = pass + 1;
+    L.n_work = static_cast<int>(work.size());
+    if ((e = cudaMemcpyAsync(ssw_work_.ptr, work.data(), work.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+      return CudaFail(e, "work list upload");
+    }
+    if (pass > 0 && (e = LaunchSswCarry(L, s)) != cudaSuccess) return CudaFail(e, "queue carry");
+    cudaMemsetAsync(counter_.ptr, 0, sizeof(int), s);
+    const int grid = std::min(L.n_work, sm_count_ * per_sm);
+    if ((e = LaunchSswWalk(L, grid, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
+    if (use_cache) {
+      for (int i = 0; i < n; ++i) {
+        const SswImage& im = imgs[static_cast<std::size_t>(i)];
+        const int wb = (pass & 1) ^ 1;
+        cudaMemsetAsync(im.g_vals[wb], 0xFF, static_cast<std::size_t>(g_cap[i]) * 4, s);
+        if (im.assoc) cudaMemsetAsync(im.g_keys[wb], 0, static_cast<std::size_t>(g_cap[i]) * 4, s);
+      }
+      if ((e = LaunchSswBuildG(L, total, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
+    }
+    cudaMemsetAsync(ssw_bad_.ptr, 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
+    if ((e = LaunchSswVerify(L, s)) != cudaSuccess) return CudaFail(e, "verification");
+    if ((e = cudaMemcpyAsync(bad.data(), ssw_bad_.ptr, static_cast<std::size_t>(n) * sizeof(int),
+                             cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+      return CudaFail(e, "verification readback");
+    }
+    int status = 0;
+    cudaMemcpy(&status, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (status != 0) {
+      cudaMemset(status_.ptr, 0, sizeof(int));
+      return Fail(RDB_E_DEVICE, "segmented walk reported status " + std::to_string(status));
+    }
+    for (int i = 0; i < n; ++i) {
+      verified[i] = std::min(bad[i], imgs[i].nsegs);
+    }
+  }
+  last_passes_ = pass;
+  return RDB_OK;
 }
 
 }  // namespace rdb

@@ -64,6 +64,7 @@ class Context {
 
  private:
   int Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int CheckJob(const rdb_job& j) const;
@@ -101,6 +102,18 @@ class Context {
   DevBuf host_in_;
   DevBuf host_idx_;
   DevBuf host_rgba_;
+  // Segmented walk.
+  DevBuf ssw_images_;
+  DevBuf ssw_segs_;
+  DevBuf ssw_work_;
+  DevBuf ssw_q_;
+  DevBuf ssw_ltab_;
+  DevBuf ssw_g_;
+  DevBuf ssw_bad_;
+  int last_passes_ = 0;
+
+ public:
+  int last_passes() const { return last_passes_; }
 };
 
 }  // namespace rdb

@@ -1,0 +1,491 @@
+// rdb_ssw.cu -- kernels of the speculative segmented walk (see rdb_ssw.h).
+//
+// The segment walker is the lane-replicated warp walker of rdb_walk_seq.cu
+// (running sums of the 15 upcoming pixels in lanes 0..14, the head pixel and
+// the last residual in every lane) extended with a start queue, a warm-up
+// prefix, an end-queue export and the segment memo described in rdb_ssw.h.
+#include <cuda_runtime.h>
+
+#include "rdb_device.cuh"
+#include "rdb_ssw.h"
+
+namespace rdb {
+namespace {
+
+constexpr int kRing = 96;
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+struct Vec4 {
+  double r, g, b, a;
+};
+
+__device__ __forceinline__ Vec4 shfl_vec(const Vec4& v, int src, bool assoc) {
+  Vec4 o;
+  o.r = __shfl_sync(0xffffffffu, v.r, src);
+  o.g = __shfl_sync(0xffffffffu, v.g, src);
+  o.b = __shfl_sync(0xffffffffu, v.b, src);
+  o.a = assoc ? __shfl_sync(0xffffffffu, v.a, src) : 0.0;
+  return o;
+}
+
+__device__ __forceinline__ Vec4 shfl_down_vec(const Vec4& v, bool assoc) {
+  Vec4 o;
+  o.r = __shfl_down_sync(0xffffffffu, v.r, 1);
+  o.g = __shfl_down_sync(0xffffffffu, v.g, 1);
+  o.b = __shfl_down_sync(0xffffffffu, v.b, 1);
+  o.a = assoc ? __shfl_down_sync(0xffffffffu, v.a, 1) : 0.0;
+  return o;
+}
+
+__device__ __forceinline__ Vec4 sample_to_vec(int assoc, float4 s) {
+  Vec4 v;
+  associate_sample(assoc, s, v.r, v.g, v.b, v.a);
+  return v;
+}
+
+__device__ __forceinline__ unsigned hash24(unsigned key) { return (key * 0x9E3779B1u) >> 8; }
+
+// ---- G: earliest first touch per key ---------------------------------------
+__device__ __forceinline__ uint32_t g_find(const SswImage& im, int buf, unsigned key) {
+  const uint32_t* vals = im.g_vals[buf];
+  const uint32_t* keys = im.g_keys[buf];
+  if (!keys) return vals[key];
+  unsigned h = hash24(key) & im.g_mask;
+#pragma unroll 1
+  for (unsigned probe = 0; probe <= im.g_mask; ++probe) {
+    const uint32_t k = keys[h];
+    if (k == key + 1u) return vals[h];
+    if (k == 0u) return kNone;
+    h = (h + 1u) & im.g_mask;
+  }
+  return kNone;
+}
+
+__device__ __forceinline__ void g_insert(const SswImage& im, int buf, unsigned key, uint32_t packed,
+                                         int* status) {
+  uint32_t* vals = im.g_vals[buf];
+  uint32_t* keys = im.g_keys[buf];
+  if (!keys) {
+    atomicMin(&vals[key], packed);
+    return;
+  }
+  unsigned h = hash24(key) & im.g_mask;
+#pragma unroll 1
+  for (unsigned probe = 0; probe <= im.g_mask; ++probe) {
+    const uint32_t old = atomicCAS(&keys[h], 0u, key + 1u);
+    if (old == 0u || old == key + 1u) {
+      atomicMin(&vals[h], packed);
+      return;
+    }
+    h = (h + 1u) & im.g_mask;
+  }
+  atomicExch(status, kDevBadPlan);  // table full: cannot happen at the sizes the host picks
+}
+
+// ---- L: one segment's keys --------------------------------------------------
+// bits 0-23 key, 24-31 the index the walk used, 32-39 the segment's own search
+// result for its first target with that key, 40-47 run tag.  The walk is
+// exact iff every used index equals what the true memo held: G's index when
+// an earlier segment touched the key first, else the segment's own result.
+__device__ __forceinline__ uint64_t l_pack(unsigned key, unsigned used, unsigned own, int tag) {
+  return static_cast<uint64_t>(key) | (static_cast<uint64_t>(used) << 24) |
+         (static_cast<uint64_t>(own) << 32) | (static_cast<uint64_t>(tag) << 40);
+}
+__device__ __forceinline__ int l_tag(uint64_t e) { return static_cast<int>((e >> 40) & 0xFFu); }
+
+// Returns the entry for `key` in this run, or 0.
+__device__ __forceinline__ uint64_t l_find(const uint64_t* tab, unsigned mask, unsigned key, int tag) {
+  unsigned h = hash24(key) & mask;
+#pragma unroll 1
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const uint64_t e = tab[h];
+    if (l_tag(e) != tag) return 0;
+    if ((e & 0xFFFFFFu) == key) return e;
+    h = (h + 1u) & mask;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ void l_insert(uint64_t* tab, unsigned mask, unsigned key, uint64_t entry,
+                                         int tag, int* status) {
+  unsigned h = hash24(key) & mask;
+#pragma unroll 1
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    if (l_tag(tab[h]) != tag) {
+      tab[h] = entry;
+      return;
+    }
+    h = (h + 1u) & mask;
+  }
+  atomicExch(status, kDevBadPlan);
+}
+
+__device__ __forceinline__ int ring_slot(int q) { return ((q >> 5) % 3) * 32 + (q & 31); }
+
+// One segment on one warp.
+template <bool kAssoc>
+__device__ void SegWalk(const SswLaunch& L, const SswImage& im, const SswSeg& sg, int sid,
+                        const PlanView& P, uint32_t* cache, int32_t* ring_ord, float4* ring_pix,
+                        int lane) {
+  const int begin = sg.begin;
+  const int end = sg.end;
+  const bool warmup = (L.pass == 0) && sg.warm > 0;
+  const int ws = warmup ? begin - sg.warm : begin;
+  const int n = end - ws;  // positions walked in this run (relative 0..n-1)
+  const int32_t* order = im.order + ws;
+  const unsigned char* img = im.pixels;
+  const int width = im.width;
+  const int layout = im.layout;
+  const int64_t stride = im.row_stride;
+  const bool use_cache = L.use_cache != 0;
+  const unsigned tag_bits = 24u - static_cast<unsigned>(L.cache_bits);
+  const unsigned tag_mask = (1u << tag_bits) - 1u;
+  uint64_t* ltab = L.ltab + (static_cast<int64_t>(sid) << L.ltab_bits);
+  const unsigned lmask = (1u << L.ltab_bits) - 1u;
+  const int gbuf = L.pass & 1;
+  const double w15 = L.sw[15];
+  const double wl = (lane < 15) ? L.sw[14 - lane] : 0.0;
+
+  // Ring preload (relative positions).
+  for (int c = 0; c < 2; ++c) {
+    const int q = 32 * c + lane;
+    int o = -1;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (q < n) {
+      o = order[q];
+      if (static_cast<unsigned>(o) >= static_cast<unsigned>(im.n)) {
+        atomicExch(L.status, kDevBadItem);
+        o = 0;
+      }
+      s = load_sample(img, layout, stride, width, o);
+    }
+    ring_ord[32 * c + lane] = o;
+    ring_pix[32 * c + lane] = s;
+  }
+  int ord_stage = (64 + lane < n) ? order[64 + lane] : -1;
+  float4 pix_stage = make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncwarp();
+
+  // Start state.  Without a warm-up the queue at `begin` comes from q_start
+  // (oldest first); with one, the walk starts at `ws` from a zero queue.
+  const double* qin = L.q_start + static_cast<int64_t>(sid) * 64;
+  Vec4 qkeep{0.0, 0.0, 0.0, 0.0};  // lane l: residual of the last position = l (mod 16)
+  Vec4 head, run, e;
+  {
+    const Vec4 p0 = sample_to_vec(kAssoc, ring_pix[0]);
+    const int qj = 1 + lane;
+    const Vec4 pj = (lane < 15 && qj < n) ? sample_to_vec(kAssoc, ring_pix[ring_slot(qj)])
+                                          : Vec4{0.0, 0.0, 0.0, 0.0};
+    head = p0;
+    run = pj;
+    e = Vec4{0.0, 0.0, 0.0, 0.0};
+    if (!warmup) {
+      // head = p_b + sum_{i<15} w_i q[i]; lane j: p_{b+1+j} + sum_{i<=13-j} w_i q[1+j+i];
+      // the pending residual is q[15].  Terms in the reference's order.
+#pragma unroll 1
+      for (int i = 0; i < 16; ++i) {
+        Vec4 qi;
+        qi.r = qin[4 * i + 0];
+        qi.g = qin[4 * i + 1];
+        qi.b = qin[4 * i + 2];
+        qi.a = qin[4 * i + 3];
+        if (i < 15) {
+          head.r = __dadd_rn(head.r, __dmul_rn(L.sw[i], qi.r));
+          head.g = __dadd_rn(head.g, __dmul_rn(L.sw[i], qi.g));
+          head.b = __dadd_rn(head.b, __dmul_rn(L.sw[i], qi.b));
+          if (kAssoc) head.a = __dadd_rn(head.a, __dmul_rn(L.sw[i], qi.a));
+        }
+        const int ti = i - 1 - lane;  // term index of q[i] for lane's pixel
+        if (lane < 15 && ti >= 0 && ti <= 13 - lane) {
+          run.r = __dadd_rn(run.r, __dmul_rn(L.sw[ti], qi.r));
+          run.g = __dadd_rn(run.g, __dmul_rn(L.sw[ti], qi.g));
+          run.b = __dadd_rn(run.b, __dmul_rn(L.sw[ti], qi.b));
+          if (kAssoc) run.a = __dadd_rn(run.a, __dmul_rn(L.sw[ti], qi.a));
+        }
+        if (i == 15) e = qi;
+        if (lane == ((begin - 16 + i) & 15)) qkeep = qi;
+      }
+    }
+  }
+  int my_index = 0;
+
+#pragma unroll 1
+  for (int t = 0; t < n; ++t) {
+    const int abs = ws + t;
+    const int phase = t & 31;
+    if (phase == 0 && t > 0) {
+      const int ch = t >> 5;
+      const int slot = ((ch + 1) % 3) * 32 + lane;
+      ring_ord[slot] = ord_stage;
+      ring_pix[slot] = pix_stage;
+      const int q2 = 32 * (ch + 2) + lane;
+      ord_stage = (q2 < n) ? order[q2] : -1;
+      __syncwarp();
+    } else if (phase == 16) {
+      if (ord_stage >= im.n) {
+        atomicExch(L.status, kDevBadItem);
+        ord_stage = 0;
+      }
+      pix_stage = (ord_stage >= 0) ? load_sample(img, layout, stride, width, ord_stage)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (warmup && abs == begin) {
+      // The queue reached at the segment start: recorded for verification.
+      if (lane < 16) {
+        const int m = (lane - (begin - 16)) & 15;
+        double* qo = L.q_start + static_cast<int64_t>(sid) * 64 + 4 * m;
+        qo[0] = qkeep.r;
+        qo[1] = qkeep.g;
+        qo[2] = qkeep.b;
+        qo[3] = qkeep.a;
+      }
+    }
+    const bool live = abs >= begin;
+
+    Vec4 v;
+    v.r = __dadd_rn(head.r, __dmul_rn(w15, e.r));
+    v.g = __dadd_rn(head.g, __dmul_rn(w15, e.g));
+    v.b = __dadd_rn(head.b, __dmul_rn(w15, e.b));
+    v.a = kAssoc ? __dadd_rn(head.a, __dmul_rn(w15, e.a)) : 0.0;
+    {
+      Vec4 rn;
+      rn.r = __dadd_rn(run.r, __dmul_rn(wl, e.r));
+      rn.g = __dadd_rn(run.g, __dmul_rn(wl, e.g));
+      rn.b = __dadd_rn(run.b, __dmul_rn(wl, e.b));
+      rn.a = kAssoc ? __dadd_rn(run.a, __dmul_rn(wl, e.a)) : 0.0;
+      head = shfl_vec(rn, 0, kAssoc);
+      run = shfl_down_vec(rn, kAssoc);
+      const int q = t + 16;
+      const Vec4 fresh = (q < n) ? sample_to_vec(kAssoc, ring_pix[ring_slot(q)])
+                                 : Vec4{0.0, 0.0, 0.0, 0.0};
+      if (lane == 14) run = fresh;
+    }
+    const float fr = clamp_pixel(v.r);
+    const float fg = clamp_pixel(v.g);
+    const float fb = clamp_pixel(v.b);
+    const float fa = kAssoc ? clamp_pixel(v.a) : 0.0f;
+    unsigned key = key6_dev(fr) | (key6_dev(fg) << 6) | (key6_dev(fb) << 12);
+    if (kAssoc) key |= key6_dev(fa) << 18;
+
+    int index = 0;
+    bool found = false;
+    const bool memo = live && use_cache;
+    unsigned h24 = 0, slot = 0;
+    if (memo) {
+      h24 = (key * 0x9E3779B1u) & 0xFFFFFFu;
+      slot = h24 >> tag_bits;
+      const unsigned ent = cache[slot];
+      index = static_cast<int>(ent & 0xFFu);
+      found = (ent >> 8) == (0x800000u | (h24 & tag_mask));
+      if (!found) {
+        const uint64_t le = l_find(ltab, lmask, key, L.tag);
+        if (le) {
+          index = static_cast<int>((le >> 24) & 0xFFu);
+          found = true;
+        }
+      }
+    }
+    if (!found) {
+      // First use of the key in this segment (or no memo): search, and take
+      // G's index instead when an earlier segment touched the key first.
+      const unsigned br = byte_dev(fr), bg = byte_dev(fg), bb = byte_dev(fb);
+      const unsigned ba = kAssoc ? byte_dev(fa) : 0u;
+      const int node = plan_descend(P, br, bg, bb, ba);
+      const Target tg = make_target(kAssoc, static_cast<double>(fr), static_cast<double>(fg),
+                                    static_cast<double>(fb), static_cast<double>(fa));
+      const int own = plan_search_warp(P, node, tg, lane);
+      index = own;
+      if (memo) {
+        const uint32_t gv = g_find(im, gbuf, key);
+        if (gv != kNone && static_cast<int>(gv >> 8) < sg.k) index = static_cast<int>(gv & 0xFFu);
+        l_insert(ltab, lmask, key, l_pack(key, index, own, L.tag), L.tag, L.status);
+      }
+    }
+    if (memo) cache[slot] = 0x80000000u | ((h24 & tag_mask) << 8) | static_cast<unsigned>(index);
+
+    const double* rc = P.rcol(index);
+    e.r = __dadd_rn(static_cast<double>(fr), -rc[0]);
+    e.g = __dadd_rn(static_cast<double>(fg), -rc[1]);
+    e.b = __dadd_rn(static_cast<double>(fb), -rc[2]);
+    e.a = kAssoc ? __dadd_rn(static_cast<double>(fa), -rc[3]) : 0.0;
+    if (lane == (abs & 15)) qkeep = e;
+
+    if (lane == phase) my_index = index;
+    if (phase == 31 || t == n - 1) {
+      const int q = (t & ~31) + lane;
+      if (q <= t && ws + q >= begin) {
+        const int rs = ring_slot(q);
+        const int o = ring_ord[rs];
+        im.indices[o] = static_cast<uint8_t>(my_index);
+        if (im.rgba_out) {
+          const float4 pc = reinterpret_cast<const float4*>(im.plan + P.h->off_out)[my_index];
+          const float a = kAssoc ? pc.w : ring_pix[rs].w;
+          im.rgba_out[o] = make_float4(pc.x, pc.y, pc.z, a);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // End queue: residuals of positions end-16 .. end-1, oldest first.
+  if (lane < 16) {
+    const int m = (lane - (end - 16)) & 15;
+    double* qo = L.q_end + static_cast<int64_t>(sid) * 64 + 4 * m;
+    qo[0] = qkeep.r;
+    qo[1] = qkeep.g;
+    qo[2] = qkeep.b;
+    qo[3] = qkeep.a;
+  }
+}
+
+__global__ void __launch_bounds__(32) SswWalkKernel(SswLaunch L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x;
+  unsigned char* plan_smem = smem;
+  const int entries = L.use_cache ? (1 << L.cache_bits) : 0;
+  uint32_t* cache = reinterpret_cast<uint32_t*>(smem + L.plan_smem_max);
+  const int ring_off = (L.plan_smem_max + 4 * entries + 15) & ~15;
+  int32_t* ring_ord = reinterpret_cast<int32_t*>(smem + ring_off);
+  float4* ring_pix = reinterpret_cast<float4*>(ring_ord + kRing);
+  const unsigned char* staged = nullptr;
+#pragma unroll 1
+  for (;;) {
+    int w = 0;
+    if (lane == 0) w = atomicAdd(L.counter, 1);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= L.n_work) break;
+    const int sid = L.work[w];
+    const SswSeg sg = L.segs[sid];
+    const SswImage& im = L.images[sg.image];
+    if (im.plan_smem > L.plan_smem_max) {
+      if (lane == 0) atomicExch(L.status, kDevBadPlan);
+      continue;
+    }
+    if (staged != im.plan) {
+      __syncwarp();
+      const int4* src = reinterpret_cast<const int4*>(im.plan);
+      int4* dst = reinterpret_cast<int4*>(plan_smem);
+      for (int i = lane; i < im.plan_smem / 16; i += 32) dst[i] = src[i];
+      staged = im.plan;
+    }
+    for (int i = lane; i < entries; i += 32) cache[i] = 0u;
+    __syncwarp();
+    PlanView P;
+    P.bind(plan_smem);
+    if (P.assoc) {
+      SegWalk<true>(L, im, sg, sid, P, cache, ring_ord, ring_pix, lane);
+    } else {
+      SegWalk<false>(L, im, sg, sid, P, cache, ring_ord, ring_pix, lane);
+    }
+    if (lane == 0) L.segs[sid].run_tag = L.tag;
+    __syncwarp();
+  }
+}
+
+// One warp per segment (every segment of every image): its own first touches
+// go into the G buffer the next pass reads.
+__global__ void SswBuildGKernel(SswLaunch L, int total) {
+  const int sid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (sid >= total) return;
+  const SswSeg sg = L.segs[sid];
+  const SswImage& im = L.images[sg.image];
+  const uint64_t* tab = L.ltab + (static_cast<int64_t>(sid) << L.ltab_bits);
+  const int cap = 1 << L.ltab_bits;
+  const int wbuf = (L.pass & 1) ^ 1;
+  for (int i = lane; i < cap; i += 32) {
+    const uint64_t e = tab[i];
+    if (l_tag(e) != sg.run_tag || sg.run_tag == 0) continue;
+    const unsigned key = static_cast<unsigned>(e & 0xFFFFFFu);
+    const uint32_t packed = (static_cast<uint32_t>(sg.k) << 8) | static_cast<uint32_t>((e >> 24) & 0xFFu);
+    g_insert(im, wbuf, key, packed, L.status);
+  }
+}
+
+// One warp per active segment.
+__global__ void SswVerifyKernel(SswLaunch L) {
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= L.n_work) return;
+  const int sid = L.work[w];
+  const SswSeg sg = L.segs[sid];
+  const SswImage& im = L.images[sg.image];
+  bool ok = true;
+  if (sg.k > 0) {
+    const double* a = L.q_start + static_cast<int64_t>(sid) * 64;
+    const double* b = L.q_end + static_cast<int64_t>(sid - 1) * 64;
+    for (int i = lane; i < 64; i += 32) {
+      if (__double_as_longlong(a[i]) != __double_as_longlong(b[i])) ok = false;
+    }
+  }
+  if (L.use_cache) {
+    const uint64_t* tab = L.ltab + (static_cast<int64_t>(sid) << L.ltab_bits);
+    const int cap = 1 << L.ltab_bits;
+    const int wbuf = (L.pass & 1) ^ 1;
+    for (int i = lane; i < cap; i += 32) {
+      const uint64_t e = tab[i];
+      if (l_tag(e) != sg.run_tag) continue;
+      const unsigned key = static_cast<unsigned>(e & 0xFFFFFFu);
+      const unsigned used = static_cast<unsigned>((e >> 24) & 0xFFu);
+      const unsigned own = static_cast<unsigned>((e >> 32) & 0xFFu);
+      const uint32_t gv = g_find(im, wbuf, key);
+      const int gseg = (gv == kNone) ? 0x7FFFFF : static_cast<int>(gv >> 8);
+      // The true memo before this segment holds the key iff an earlier
+      // segment touched it (every earlier segment is exact when this one is
+      // judged); the walk must have used that index, else its own result.
+      const unsigned truth = (gseg < sg.k) ? (gv & 0xFFu) : own;
+      if (used != truth) ok = false;
+    }
+  }
+  const bool all = __all_sync(0xffffffffu, ok);
+  if (!all && lane == 0) atomicMin(&L.first_bad[sg.image], sg.k);
+}
+
+__global__ void SswCarryKernel(SswLaunch L) {
+  const int w = blockIdx.x;
+  if (w >= L.n_work) return;
+  const int sid = L.work[w];
+  const SswSeg sg = L.segs[sid];
+  if (sg.k == 0) return;
+  const int i = threadIdx.x;
+  if (i < 64) {
+    L.q_start[static_cast<int64_t>(sid) * 64 + i] = L.q_end[static_cast<int64_t>(sid - 1) * 64 + i];
+  }
+}
+
+}  // namespace
+
+std::size_t SswSmemBytes(int plan_smem_max, int cache_bits) {
+  const std::size_t ring_off = (static_cast<std::size_t>(plan_smem_max) +
+                                (static_cast<std::size_t>(4) << cache_bits) + 15) &
+                               ~static_cast<std::size_t>(15);
+  return ring_off + kRing * (sizeof(int32_t) + sizeof(float4));
+}
+
+cudaError_t LaunchSswWalk(const SswLaunch& L, int grid, cudaStream_t s) {
+  const std::size_t smem = SswSmemBytes(L.plan_smem_max, L.cache_bits);
+  cudaError_t e = cudaFuncSetAttribute(SswWalkKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  SswWalkKernel<<<grid, 32, smem, s>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchSswBuildG(const SswLaunch& L, int total_segs, cudaStream_t s) {
+  if (total_segs <= 0 || !L.use_cache) return cudaSuccess;
+  SswBuildGKernel<<<(total_segs + 7) / 8, 256, 0, s>>>(L, total_segs);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchSswVerify(const SswLaunch& L, cudaStream_t s) {
+  if (L.n_work <= 0) return cudaSuccess;
+  SswVerifyKernel<<<(L.n_work + 7) / 8, 256, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchSswCarry(const SswLaunch& L, cudaStream_t s) {
+  if (L.n_work <= 0) return cudaSuccess;
+  SswCarryKernel<<<L.n_work, 64, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
+}  // namespace rdb
