@@ -83,6 +83,10 @@ int rdb_context_create(int device, size_t memory_budget, rdb_context** out);
 void rdb_context_destroy(rdb_context* ctx);
 /* Device bytes currently held by the context. */
 size_t rdb_context_bytes(const rdb_context* ctx);
+/* Passes the last segmented sequential walk on this context took (0 before
+ * any; 1 when every segment's speculation held on the first pass).  No
+ * reference counterpart: the reference walks one chain. */
+int rdb_context_last_passes(const rdb_context* ctx);
 
 /* A palette and its colour tree, in the reference's own terms
  * (rd::Palette, include/rd_riemersma.h:63-67; rd::QNode, include/rd_octree.h:43-52). */
@@ -107,6 +111,13 @@ int rdb_palette_create(rdb_context* ctx, const rdb_palette_desc* desc, int* pale
 int rdb_plan_build(const rdb_palette_desc* desc, void* out, size_t cap, size_t* size);
 int rdb_palette_from_octree(rdb_context* ctx, const rdb_octree* t, int* palette_id);
 int rdb_palette_destroy(rdb_context* ctx, int palette_id);
+/* The palette's uniform-key table (stipple_b200/csrc/rdb_uniform.h) copied to
+ * host memory: 2^18 bytes, one per 6-bit-per-channel memo key, holding the
+ * colour number every target with that key receives, or 255 when the search
+ * result can vary inside the key (or is colour 255).  Palettes without
+ * associated alpha only.  No reference counterpart: it is how the sequential
+ * engines skip the memo for such keys. */
+int rdb_palette_uniform(rdb_context* ctx, int palette_id, uint8_t* out, size_t cap);
 
 /* ---- dithering -----------------------------------------------------------
  * One image.  Device pointers. */
@@ -131,7 +142,11 @@ typedef struct rdb_options {
   int jacobi_fp64;      /* default 0 (ApproxOptions::fp64) */
   int cache_bits;       /* sequential engine: log2 shared-memory memo cache entries, 0 = auto */
   int seq_mode;         /* sequential engine: 0 = auto, 1 = one warp walks each image whole,
-                           2 = speculative segmented walk (exact; see rdb_ssw.h) */
+                           2 = speculative segmented walk on warps (exact; rdb_ssw.h),
+                           3 = the same on thread walkers, palettes without associated
+                           alpha only (exact; rdb_tsw.h).  Auto: images under 8192
+                           pixels mode 1, alpha-associated palettes mode 2, others 3.
+                           The segmented modes wait for the stream between passes. */
   int seg_len;          /* segmented walk: positions per segment, 0 = auto */
   int warm_len;         /* segmented walk: warm-up positions before each segment, 0 = auto */
   int max_passes;       /* segmented walk: give up after this many passes (0 = no limit); the

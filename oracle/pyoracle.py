@@ -140,6 +140,19 @@ class Oracle:
         return Tree(cm, child, parent, cn, nu, t.depth, bool(t.associate_alpha))
 
     # -- walks ---------------------------------------------------------------
+    def lookups(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
+                targets: np.ndarray) -> np.ndarray:
+        """Builds the palette, then the reference lookup (descent + ClosestColor,
+        src/rd_riemersma_cpu.cpp:82-92) of each clamped target row (r, g, b, a)."""
+        t = self.build_tree_raw(rgbaf, max_colors, assoc, gray)
+        try:
+            out = np.empty(len(targets), np.int32)
+            for i, (r, g, b, a) in enumerate(np.asarray(targets, np.float64)):
+                out[i] = self.lib.orc_tree_lookup(C.byref(t), float(r), float(g), float(b), float(a))
+            return out
+        finally:
+            self.lib.orc_tree_free(C.byref(t))
+
     def walk_seq(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
                  diffusion: float = 1.0, use_cache: bool = True):
         """Builds the palette, then the sequential walk.  Returns (idx, out, palette)."""

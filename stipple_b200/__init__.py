@@ -98,11 +98,13 @@ SIGNATURES = {
     "rdb_context_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
     "rdb_context_destroy": (None, [C.c_void_p]),
     "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
+    "rdb_context_last_passes": (C.c_int, [C.c_void_p]),
     "rdb_palette_create": (C.c_int, [C.c_void_p, C.POINTER(PaletteDesc), C.POINTER(C.c_int)]),
     "rdb_palette_from_octree": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "rdb_plan_build": (C.c_int, [C.POINTER(PaletteDesc), C.c_void_p, C.c_size_t,
                                  C.POINTER(C.c_size_t)]),
     "rdb_palette_destroy": (C.c_int, [C.c_void_p, C.c_int]),
+    "rdb_palette_uniform": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "rdb_options_default": (None, [C.POINTER(Options)]),
     "rdb_dither": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Job), C.c_int, C.POINTER(Options),
                              C.c_void_p]),
@@ -235,6 +237,11 @@ class Context:
     def bytes(self) -> int:
         return load().rdb_context_bytes(self.handle)
 
+    @property
+    def last_passes(self) -> int:
+        """Passes the last segmented sequential walk took."""
+        return load().rdb_context_last_passes(self.handle)
+
     # -- palettes ---------------------------------------------------------
     def palette_from_octree(self, tree: Octree) -> int:
         pid = C.c_int()
@@ -257,6 +264,12 @@ class Context:
 
     def release_palette(self, pid: int) -> None:
         _check(load().rdb_palette_destroy(self.handle, pid))
+
+    def uniform_table(self, pid: int) -> np.ndarray:
+        """The palette's uniform-key table: 2^18 bytes, 255 = not uniform."""
+        out = np.empty(1 << 18, np.uint8)
+        _check(load().rdb_palette_uniform(self.handle, pid, _ptr(out), out.nbytes))
+        return out
 
     # -- dithering (host buffers) ----------------------------------------
     def dither_host(self, engine: str | int, images, palette_ids, rgba: bool = False,

@@ -41,6 +41,8 @@ SOURCES = [
     "rdb_walk_blocks.cu",
     "rdb_jacobi.cu",
     "rdb_ssw.cu",
+    "rdb_tsw.cu",
+    "rdb_uniform.cu",
 ]
 
 

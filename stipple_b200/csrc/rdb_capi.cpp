@@ -10,6 +10,7 @@
 #include "rdb_numeric.h"
 #include "rdb_octree.h"
 #include "rdb_runtime.h"
+#include "rdb_uniform.h"
 
 struct rdb_octree {
   rdb::Octree tree;
@@ -151,6 +152,8 @@ void rdb_context_destroy(rdb_context* ctx) { delete ctx; }
 
 size_t rdb_context_bytes(const rdb_context* ctx) { return ctx ? ctx->impl.bytes() : 0; }
 
+int rdb_context_last_passes(const rdb_context* ctx) { return ctx ? ctx->impl.last_passes() : 0; }
+
 int rdb_palette_create(rdb_context* ctx, const rdb_palette_desc* d, int* palette_id) {
   if (!ctx || !d || !palette_id || !d->colors || !d->child || !d->color_number ||
       !d->number_unique) {
@@ -224,6 +227,18 @@ int rdb_palette_from_octree(rdb_context* ctx, const rdb_octree* t, int* palette_
 int rdb_palette_destroy(rdb_context* ctx, int palette_id) {
   if (!ctx) return Guard("rdb_palette_destroy");
   return ctx->impl.DestroyPalette(palette_id);
+}
+
+int rdb_palette_uniform(rdb_context* ctx, int palette_id, uint8_t* out, size_t cap) {
+  if (!ctx || !out) return Guard("rdb_palette_uniform");
+  if (cap < static_cast<size_t>(rdb::kUniformKeys)) {
+    return rdb::Fail(RDB_E_INVALID, "rdb_palette_uniform: buffer shorter than 2^18 bytes");
+  }
+  cudaSetDevice(ctx->impl.device());
+  const uint8_t* dev = nullptr;
+  if (int rc = ctx->impl.Uniform(palette_id, ctx->impl.stream(), &dev)) return rc;
+  const cudaError_t e = cudaMemcpy(out, dev, rdb::kUniformKeys, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? RDB_OK : rdb::CudaFail(e, "rdb_palette_uniform");
 }
 
 void rdb_options_default(rdb_options* o) {

@@ -8,6 +8,8 @@
 #include "rdb_curve.h"
 #include "rdb_numeric.h"
 #include "rdb_ssw.h"
+#include "rdb_tsw.h"
+#include "rdb_uniform.h"
 
 namespace rdb {
 namespace {
@@ -40,12 +42,17 @@ int CudaFail(cudaError_t e, const char* what) {
 Context::~Context() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
-  for (auto& p : plans_) cudaFree(p.second.dev);
+  for (auto& p : plans_) {
+    cudaFree(p.second.dev);
+    cudaFree(p.second.uniform);
+  }
   for (auto& o : orders_) cudaFree(o.second);
   for (DevBuf* b : {&memo_, &memo_gen_, &seq_items_, &counter_, &status_, &curve_scratch_,
                     &block_images_, &block_offsets_, &block_cx_, &block_chosen_, &jac_cx_,
                     &jac_q_, &jac_g_, &host_in_, &host_idx_, &host_rgba_, &ssw_images_,
-                    &ssw_segs_, &ssw_work_, &ssw_q_, &ssw_ltab_, &ssw_g_, &ssw_bad_}) {
+                    &ssw_segs_, &ssw_work_, &ssw_q_, &ssw_ltab_, &ssw_g_, &ssw_bad_,
+                    &tsw_images_, &tsw_chunks_, &tsw_bad_, &tsw_q_, &tsw_own_, &tsw_list_,
+                    &tsw_count_, &tsw_cx_, &tsw_chosen_, &tsw_g_}) {
     Release(b);
   }
   if (stream_) cudaStreamDestroy(stream_);
@@ -141,7 +148,35 @@ int Context::DestroyPalette(int id) {
   cudaStreamSynchronize(stream_);
   cudaFree(it->second.dev);
   bytes_ -= it->second.host.size();
+  if (it->second.uniform) {
+    cudaDeviceSynchronize();  // any stream may still read it
+    cudaFree(it->second.uniform);
+    bytes_ -= kUniformKeys;
+  }
   plans_.erase(it);
+  return RDB_OK;
+}
+
+int Context::Uniform(int id, cudaStream_t s, const uint8_t** out) {
+  auto it = plans_.find(id);
+  if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
+  DevPlan& p = it->second;
+  if (p.assoc) return Fail(RDB_E_UNSUPPORTED, "uniform-key table: alpha-associated palette");
+  if (!p.uniform) {
+    if (bytes_ + kUniformKeys > budget_) return Fail(RDB_E_NOMEM, "uniform-key table: budget exceeded");
+    cudaError_t e = cudaMalloc(&p.uniform, kUniformKeys);
+    if (e != cudaSuccess) {
+      p.uniform = nullptr;
+      return CudaFail(e, "uniform-key table");
+    }
+    bytes_ += kUniformKeys;
+    // Built once; other streams may read it later, so it is complete on return.
+    if ((e = LaunchUniformTable(p.dev, p.uniform, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+      return CudaFail(e, "uniform-key table");
+    }
+  }
+  *out = p.uniform;
   return RDB_OK;
 }
 
@@ -238,10 +273,9 @@ int Context::Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o
     case RDB_ENGINE_SEQ: {
       if (o.seq_mode == 1) return Seq(jobs, n, o, s);
       if (o.seq_mode == 2) return SeqSegmented(jobs, n, o, s);
-      // Automatic: segment once any image is long enough to split.
-      int64_t longest = 0;
-      for (int i = 0; i < n; ++i) longest = std::max<int64_t>(longest, int64_t{jobs[i].width} * jobs[i].height);
-      return longest >= 8192 ? SeqSegmented(jobs, n, o, s) : Seq(jobs, n, o, s);
+      if (o.seq_mode == 3) return SeqThreadSegmented(jobs, n, o, s);
+      if (o.seq_mode != 0) return Fail(RDB_E_INVALID, "seq_mode must be 0..3");
+      return SeqAuto(jobs, n, o, s);
     }
     case RDB_ENGINE_BLOCKS: return Blocks(jobs, n, o, s);
     case RDB_ENGINE_JACOBI: return Jacobi(jobs, n, o, s);
@@ -765,6 +799,197 @@ int Context::SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cuda
     }
   }
   last_passes_ = pass;
+  return RDB_OK;
+}
+
+// Automatic sequential mode: short images walk whole on one warp each, long
+// ones are segmented -- on thread walkers unless the palette associates alpha.
+int Context::SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  std::vector<rdb_job> plain, warp, thread;
+  for (int i = 0; i < n; ++i) {
+    const rdb_job& j = jobs[i];
+    const int64_t px = int64_t{j.width} * j.height;
+    if (px < 8192) {
+      plain.push_back(j);
+    } else if (Plan(j.palette_id)->assoc) {
+      warp.push_back(j);
+    } else {
+      thread.push_back(j);
+    }
+  }
+  if (!plain.empty()) {
+    if (int rc = Seq(plain.data(), static_cast<int>(plain.size()), o, s)) return rc;
+  }
+  if (!warp.empty()) {
+    if (int rc = SeqSegmented(warp.data(), static_cast<int>(warp.size()), o, s)) return rc;
+  }
+  if (!thread.empty()) {
+    if (int rc = SeqThreadSegmented(thread.data(), static_cast<int>(thread.size()), o, s)) return rc;
+  }
+  return RDB_OK;
+}
+
+// The thread-walker segmented walk (rdb_tsw.h): every image's visit order is
+// cut into segments of seg_len positions, one thread each; passes repeat
+// until each image's verified prefix covers it.
+int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  const bool use_cache = o.use_cache != 0;
+  int seg_len = o.seg_len > 0 ? std::max(o.seg_len, 64) : 256;
+  seg_len = (seg_len + 15) & ~15;
+  const int warm_len = std::max(16, o.warm_len > 0 ? o.warm_len : 128);
+  constexpr int kChunk = 128;
+  constexpr int kKeys = 1 << 18;
+  std::vector<TswImage> imgs(static_cast<std::size_t>(n));
+  std::vector<TswChunk> chunks;
+  int plan_max = 0;
+  bool is_float = false;
+  int total = 0;
+  int64_t positions = 0;
+  for (int i = 0; i < n; ++i) {
+    const rdb_job& j = jobs[i];
+    const DevPlan* p = Plan(j.palette_id);
+    if (p->assoc) return Fail(RDB_E_UNSUPPORTED, "thread segmented walk: alpha-associated palette");
+    const int32_t* order = nullptr;
+    if (int rc = Order(j.width, j.height, s, &order)) return rc;
+    TswImage& im = imgs[static_cast<std::size_t>(i)];
+    std::memset(&im, 0, sizeof(im));
+    im.pixels = static_cast<const unsigned char*>(j.pixels);
+    im.row_stride = static_cast<int64_t>(RowStride(j));
+    im.width = j.width;
+    im.height = j.height;
+    im.layout = j.layout;
+    im.n = j.width * j.height;
+    im.order = order;
+    im.indices = j.indices;
+    im.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+    im.plan = p->dev;
+    im.plan_smem = p->smem;
+    if (int rc = Uniform(j.palette_id, s, &im.uni)) return rc;
+    im.first_seg = total;
+    im.nsegs = (im.n + seg_len - 1) / seg_len;
+    im.cx_offset = positions;
+    for (int k0 = 0; k0 < im.nsegs; k0 += kChunk) {
+      chunks.push_back(TswChunk{i, k0, std::min(kChunk, im.nsegs - k0), 0});
+    }
+    total += im.nsegs;
+    positions += (im.n + 15) & ~15;
+    plan_max = std::max(plan_max, p->smem);
+    is_float = is_float || j.layout == RDB_RGBAF32;
+  }
+  if (static_cast<std::size_t>(plan_max) > smem_optin_) {
+    return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
+  }
+  int own_bits = 4;
+  while ((1 << own_bits) < 2 * seg_len) ++own_bits;
+  const std::size_t own_entries = static_cast<std::size_t>(total) << own_bits;
+  const std::size_t q_bytes = static_cast<std::size_t>(total) * 64 * sizeof(double);
+  const std::size_t g_words = static_cast<std::size_t>(n) * 3 * kKeys;
+  if (int rc = Reserve(&tsw_images_, imgs.size() * sizeof(TswImage), "segmented walk images")) return rc;
+  if (int rc = Reserve(&tsw_chunks_, chunks.size() * sizeof(TswChunk), "segment chunks")) return rc;
+  if (int rc = Reserve(&tsw_bad_, 2 * static_cast<std::size_t>(n) * sizeof(int), "verification flags")) return rc;
+  if (int rc = Reserve(&tsw_q_, 3 * q_bytes, "segment queues")) return rc;
+  if (int rc = Reserve(&tsw_cx_, static_cast<std::size_t>(positions) * (is_float ? 16 : 4), "gathered samples")) return rc;
+  if (int rc = Reserve(&tsw_chosen_, static_cast<std::size_t>(positions), "segment indices")) return rc;
+  if (use_cache) {
+    if (int rc = Reserve(&tsw_own_, own_entries * sizeof(uint64_t), "segment memo tables")) return rc;
+    if (int rc = Reserve(&tsw_list_, own_entries * sizeof(uint32_t), "segment memo lists")) return rc;
+    if (int rc = Reserve(&tsw_count_, static_cast<std::size_t>(total) * sizeof(int), "segment memo counts")) return rc;
+    if (int rc = Reserve(&tsw_g_, g_words * sizeof(uint32_t), "first-touch maps")) return rc;
+    uint32_t* g = static_cast<uint32_t*>(tsw_g_.ptr);
+    for (int i = 0; i < n; ++i) {
+      TswImage& im = imgs[static_cast<std::size_t>(i)];
+      uint32_t* base = g + static_cast<std::size_t>(i) * 3 * kKeys;
+      im.g[0] = base;
+      im.g[1] = base + kKeys;
+      im.usemin = base + 2 * static_cast<std::size_t>(kKeys);
+    }
+  }
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(tsw_images_.ptr, imgs.data(), imgs.size() * sizeof(TswImage),
+                           cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(tsw_chunks_.ptr, chunks.data(), chunks.size() * sizeof(TswChunk),
+                           cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+    return CudaFail(e, "segment upload");
+  }
+  int* bad = static_cast<int*>(tsw_bad_.ptr);
+  TswLaunch L{};
+  L.images = static_cast<const TswImage*>(tsw_images_.ptr);
+  L.n_images = n;
+  L.chunks = static_cast<const TswChunk*>(tsw_chunks_.ptr);
+  L.n_chunks = static_cast<int>(chunks.size());
+  L.seg_len = seg_len;
+  L.warm_len = warm_len;
+  L.q_start = static_cast<double*>(tsw_q_.ptr);
+  L.q_end[0] = L.q_start + static_cast<std::size_t>(total) * 64;
+  L.q_end[1] = L.q_end[0] + static_cast<std::size_t>(total) * 64;
+  L.own = static_cast<uint64_t*>(tsw_own_.ptr);
+  L.own_list = static_cast<uint32_t*>(tsw_list_.ptr);
+  L.own_count = static_cast<int*>(tsw_count_.ptr);
+  L.own_bits = own_bits;
+  L.cx = tsw_cx_.ptr;
+  L.chosen = static_cast<uint8_t*>(tsw_chosen_.ptr);
+  L.use_cache = use_cache ? 1 : 0;
+  L.is_float = is_float ? 1 : 0;
+  L.plan_smem_max = plan_max;
+  L.chunk_threads = kChunk;
+  L.bad[0] = bad;
+  L.bad[1] = bad + n;
+  L.status = static_cast<int*>(status_.ptr);
+  scaled_weights(o.diffusion, L.sw);
+
+  // Pass 0 reads bad[1] as "nothing verified" and g[1] as the empty map.
+  cudaMemsetAsync(L.bad[1], 0, static_cast<std::size_t>(n) * sizeof(int), s);
+  if (use_cache) {
+    cudaMemsetAsync(tsw_own_.ptr, 0, own_entries * sizeof(uint64_t), s);
+    for (int i = 0; i < n; ++i) {
+      cudaMemsetAsync(imgs[static_cast<std::size_t>(i)].g[1], 0xFF, kKeys * sizeof(uint32_t), s);
+    }
+  }
+  if ((e = LaunchTswGather(L, positions, s)) != cudaSuccess) return CudaFail(e, "sample gather");
+
+  std::vector<int> bad_h(static_cast<std::size_t>(n));
+  std::vector<int> front(static_cast<std::size_t>(n), -1);
+  const int max_passes = o.max_passes > 0 ? o.max_passes : 1 << 30;
+  int pass = 0;
+  for (;; ++pass) {
+    if (pass >= max_passes) {
+      return Fail(RDB_E_DEVICE, "segmented walk did not converge within the pass limit");
+    }
+    L.pass = pass;
+    L.tag = static_cast<uint32_t>(pass + 1);
+    int* cur = L.bad[pass & 1];
+    cudaMemsetAsync(cur, 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
+    if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
+    if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
+    if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
+    if ((e = cudaMemcpyAsync(bad_h.data(), cur, static_cast<std::size_t>(n) * sizeof(int),
+                             cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+      return CudaFail(e, "verification readback");
+    }
+    int status = 0;
+    cudaMemcpy(&status, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (status != 0) {
+      cudaMemset(status_.ptr, 0, sizeof(int));
+      return Fail(RDB_E_DEVICE, "segmented walk reported status " + std::to_string(status));
+    }
+    // The verified prefix of every unfinished image grows by at least one
+    // segment a pass (its first walked segment started from exact state);
+    // anything else is an engine fault, reported rather than looped on.
+    bool done = true;
+    for (int i = 0; i < n; ++i) {
+      const std::size_t si = static_cast<std::size_t>(i);
+      const int nf = std::min(bad_h[si], imgs[si].nsegs);
+      if (nf < imgs[si].nsegs && nf <= front[si]) {
+        return Fail(RDB_E_DEVICE, "segmented walk made no progress on an image");
+      }
+      front[si] = nf;
+      done = done && nf >= imgs[si].nsegs;
+    }
+    if (done) break;
+  }
+  last_passes_ = pass + 1;
+  if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
   return RDB_OK;
 }
 

@@ -36,6 +36,7 @@ struct DevPlan {
   int smem = 0;
   int count = 0;
   bool assoc = false;
+  uint8_t* uniform = nullptr;  // uniform-key table (rdb_uniform.h), built on first use
 };
 
 class Context {
@@ -46,6 +47,8 @@ class Context {
   int CreatePalette(const PlanInput& in, int* id);
   int DestroyPalette(int id);
   const DevPlan* Plan(int id) const;
+  // The palette's uniform-key table, built on the stream on first use.
+  int Uniform(int id, cudaStream_t s, const uint8_t** out);
 
   // Visit order of a geometry, built on first use and kept resident.
   int Order(int width, int height, cudaStream_t s, const int32_t** out);
@@ -65,6 +68,8 @@ class Context {
  private:
   int Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int CheckJob(const rdb_job& j) const;
@@ -110,6 +115,17 @@ class Context {
   DevBuf ssw_ltab_;
   DevBuf ssw_g_;
   DevBuf ssw_bad_;
+  // Thread-walker segmented walk.
+  DevBuf tsw_images_;
+  DevBuf tsw_chunks_;
+  DevBuf tsw_bad_;
+  DevBuf tsw_q_;
+  DevBuf tsw_own_;
+  DevBuf tsw_list_;
+  DevBuf tsw_count_;
+  DevBuf tsw_cx_;
+  DevBuf tsw_chosen_;
+  DevBuf tsw_g_;
   int last_passes_ = 0;
 
  public:

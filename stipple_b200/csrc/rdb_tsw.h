@@ -1,0 +1,107 @@
+// rdb_tsw.h -- the speculative segmented walk on thread walkers: one thread
+// per segment, for palettes without associated alpha.
+//
+// The exactness argument is the one of rdb_ssw.h (segments replayed from
+// guessed states, checked against their predecessors, a verified prefix that
+// grows by at least one segment a pass); what changes is the bookkeeping,
+// which no longer keeps a per-segment table of every key touched:
+//
+//   G_prev  the previous pass's first-touch map, (segment << 8 | index) per
+//           6-bit key, 0xFFFFFFFF = untouched.  A segment k answers a key from
+//           G_prev whenever G_prev names an earlier segment, and then records
+//           only "k took this key from G" (usemin[key] = min k).
+//   own     keys G_prev gives no earlier segment for are searched by the
+//           segment itself on first use and memoised in its own table (the
+//           reference's first-touch rule, rd_types.h:111-153, inside the
+//           segment); each such first use is also appended to the segment's
+//           own list.
+//   G_new   every touch does atomicMin(G_new[key], k << 8 | index).  G_new
+//           starts as G_prev with only the entries of verified segments kept,
+//           so after the walk it is the first-touch map of this pass.
+//
+// Checks after the walk, all of which must hold for a segment to be exact
+// given exact predecessors:
+//   queue   its start queue equals its predecessor's end queue bit for bit;
+//   from G  for every key with usemin = u: G_new still names a segment before
+//           u and with the index G_prev gave (the earliest taker fails first,
+//           so u alone decides the verified prefix);
+//   own     for every own first use (key, index) of segment k: no earlier
+//           segment touched the key in G_new, or it gave the same index.
+// The first failing segment per image bounds the next verified prefix.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace rdb {
+
+struct TswImage {
+  const unsigned char* pixels;
+  int64_t row_stride;
+  int width;
+  int height;
+  int layout;                // 3, 4 (8-bit) or 16 (float4 Q16)
+  int n;                     // positions (= pixels)
+  const int32_t* order;      // sequential visit order
+  uint8_t* indices;
+  float4* rgba_out;
+  const unsigned char* plan; // device plan blob
+  const uint8_t* uni;        // uniform-key table of the palette (rdb_uniform.h)
+  int plan_smem;
+  int first_seg;             // global id of segment 0
+  int nsegs;
+  int64_t cx_offset;         // first position in the gathered sample / index buffers
+  uint32_t* g[2];            // first-touch maps (2^18 entries each); pass p writes g[p & 1]
+  uint32_t* usemin;          // 2^18: earliest segment that took the key from G_prev
+};
+
+// A CTA's work: segments k0 .. k0 + count - 1 of one image (one plan per CTA).
+struct TswChunk {
+  int image;
+  int k0;
+  int count;
+  int pad;
+};
+
+struct TswLaunch {
+  const TswImage* images;
+  int n_images;
+  const TswChunk* chunks;
+  int n_chunks;
+  int pass;
+  uint32_t tag;              // own-table tag of this pass (nonzero)
+  int seg_len;
+  int warm_len;
+  double* q_start;           // per segment, pass 0: queue at its start after the warm-up
+  double* q_end[2];          // per segment, by pass parity: 16 x 4 doubles, oldest first
+  uint64_t* own;             // per segment: 2^own_bits entries (key | index << 24 | tag << 32)
+  uint32_t* own_list;        // per segment: 2^own_bits words (key | index << 24)
+  int* own_count;            // per segment
+  int own_bits;
+  const void* cx;            // gathered samples: uint32 RGBA8 or float4 per position
+  uint8_t* chosen;           // per position
+  int use_cache;
+  int is_float;
+  int plan_smem_max;
+  int chunk_threads;
+  // Per image, by pass parity: the first failing segment of that pass (large
+  // = none).  Pass p walks from min(bad[(p-1) & 1], nsegs) -- its verified
+  // prefix -- and writes bad[p & 1].
+  int* bad[2];
+  int* status;
+  double sw[16];
+};
+
+std::size_t TswSmemBytes(int plan_smem_max);
+// Samples of every image in visit order, into L.cx.
+cudaError_t LaunchTswGather(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
+// G_new = verified entries of G_prev, usemin cleared (memo only).
+cudaError_t LaunchTswPrepare(const TswLaunch& L, cudaStream_t s);
+cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s);
+// The three checks; the first failing segment per image into L.bad[pass & 1].
+cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s);
+// Indices (and RgbaF output) of every position into the images.
+cudaError_t LaunchTswScatter(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
+
+}  // namespace rdb

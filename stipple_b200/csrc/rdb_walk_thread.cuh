@@ -108,5 +108,51 @@ __device__ __forceinline__ int search(const Plan& P, int node, double tr, double
   return slot < 0 ? 0 : static_cast<int>(P.seq[slot]);
 }
 
+// The same search spread over the 32 lanes of a warp for ONE target (every
+// lane passes the same node and target): lane l scans slots start+l,
+// start+l+32, ..., keeping its last minimum; the butterfly then keeps the
+// smaller distance and, between equal distances, the later slot -- the
+// reference's "last equal minimum in post-order" rule.  All 32 lanes must
+// call it together.
+template <bool kAssoc>
+__device__ __forceinline__ int search_warp(const Plan& P, int node, double tr, double tg,
+                                           double tb, double ta, int lane) {
+  const int start = P.range[2 * node];
+  const int len = P.range[2 * node + 1];
+  const double* dr = P.slotpal;
+  const double* dg = dr + P.slot_stride;
+  const double* db = dg + P.slot_stride;
+  const double* da = db + P.slot_stride;
+  double best = kSearchStart;
+  int slot = -1;
+#pragma unroll 1
+  for (int s = start + lane; s < start + len; s += 32) {
+    const double x = __dadd_rn(dr[s], -tr);
+    const double y = __dadd_rn(dg[s], -tg);
+    const double z = __dadd_rn(db[s], -tb);
+    double d = __dmul_rn(x, x);
+    d = __dadd_rn(d, __dmul_rn(y, y));
+    d = __dadd_rn(d, __dmul_rn(z, z));
+    if (kAssoc) {
+      const double w = __dadd_rn(da[s], -ta);
+      d = __dadd_rn(d, __dmul_rn(w, w));
+    }
+    if (d <= best) {
+      best = d;
+      slot = s;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+    const int os = __shfl_xor_sync(0xffffffffu, slot, off);
+    if (ob < best || (ob == best && os > slot)) {
+      best = ob;
+      slot = os;
+    }
+  }
+  return slot < 0 ? 0 : static_cast<int>(P.seq[slot]);
+}
+
 }  // namespace tw
 }  // namespace rdb

@@ -1,0 +1,122 @@
+"""The segmented walk on thread walkers (seq_mode=3): bit-exact with the
+reference CPU walk for every segmentation, memo table included.  Short
+segments and warm-ups force many passes, so the three checks and the pass
+loop are exercised, not only the first pass."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import stipple_b200 as sb
+from stipple_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("seg,warm", [(64, 16), (256, 128), (1024, 512)])
+def test_thread_segmented_matches_oracle(ctx, oracle, seg, warm):
+    for k, (w, h, colors) in enumerate([(256, 192, 16), (300, 211, 256), (97, 403, 64)]):
+        img = synth.gradient_rgb8(w, h, 40 + k)
+        t = sb.Octree(img, colors, False)
+        pid = ctx.palette_from_octree(t)
+        try:
+            got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=seg, warm_len=warm)
+            want, _, _ = oracle.walk_seq(synth.to_q16(img), colors, False, t.grayscale)
+            assert np.array_equal(got, want), (w, h, colors, seg, warm)
+            assert ctx.last_passes >= 1
+        finally:
+            ctx.release_palette(pid)
+
+
+def test_thread_segmented_no_cache_and_diffusion(ctx, oracle):
+    img = synth.gradient_rgb8(400, 300, 8)
+    t = sb.Octree(img, 32, False)
+    pid = ctx.palette_from_octree(t)
+    q = synth.to_q16(img)
+    try:
+        for cache in (0, 1):
+            for diff in (0.5, 1.0):
+                got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=128, warm_len=32,
+                                      use_cache=cache, diffusion=diff)
+                want, _, _ = oracle.walk_seq(q, 32, False, False, diffusion=diff, use_cache=bool(cache))
+                assert np.array_equal(got, want), (cache, diff)
+    finally:
+        ctx.release_palette(pid)
+
+
+def test_thread_segmented_gray_and_float(ctx, oracle):
+    """A greyscale palette (the deepest tree, whose descent reads bits below the
+    memo key) and RgbaF input that is not 8-bit multiples."""
+    img = synth.gradient_rgb8(320, 200, 12)
+    g = img[..., :1].repeat(3, axis=2).copy()
+    t = sb.Octree(g, 16, False)
+    assert t.grayscale
+    pid = ctx.palette_from_octree(t)
+    try:
+        got = ctx.dither_host("seq", g, pid, seq_mode=3, seg_len=128, warm_len=64)
+        want, _, _ = oracle.walk_seq(synth.to_q16(g), 16, False, True)
+        assert np.array_equal(got, want)
+    finally:
+        ctx.release_palette(pid)
+    rng = np.random.default_rng(3)
+    q = (rng.random((150, 190, 4)) * 65535.0).astype(np.float32)
+    q[..., 3] = 65535.0
+    tree = oracle.build_tree(q, 64, False, False)
+    pid = ctx.palette(tree.palette, tree.child, tree.color_number, tree.number_unique, False,
+                      parent=tree.parent)
+    try:
+        got = ctx.dither_host("seq", q, pid, seq_mode=3, seg_len=256, warm_len=64)
+        want, _, _ = oracle.walk_seq(q, 64, False, False)
+        assert np.array_equal(got, want)
+    finally:
+        ctx.release_palette(pid)
+
+
+def test_thread_segmented_batch_rgba_out(ctx, oracle):
+    """Uneven images in one call, RgbaF output included; each image is the
+    same as alone."""
+    sizes = [(1, 1), (3, 5), (17, 13), (640, 64), (129, 257), (512, 480), (64, 64)]
+    imgs, pids, want = [], [], []
+    for k, (w, h) in enumerate(sizes):
+        img = synth.gradient_rgb8(w, h, 70 + k) if k % 2 else synth.gradient_rgba8(w, h, 70 + k)
+        colors = [16, 256, 8, 64, 2, 256, 4][k]
+        t = sb.Octree(img, colors, False)
+        pids.append(ctx.palette_from_octree(t))
+        imgs.append(img)
+        want.append(oracle.walk_seq(synth.to_q16(img), colors, False, t.grayscale))
+    try:
+        got, rgba = ctx.dither_host("seq", imgs, pids, rgba=True, seq_mode=3, seg_len=128,
+                                    warm_len=64)
+        for k in range(len(imgs)):
+            assert np.array_equal(got[k], want[k][0]), sizes[k]
+            _, out, _ = want[k]
+            assert np.array_equal(rgba[k][..., :3], out[..., :3]), sizes[k]
+            solo = ctx.dither_host("seq", imgs[k], pids[k], seq_mode=3, seg_len=128, warm_len=64)
+            assert np.array_equal(solo, got[k]), sizes[k]
+    finally:
+        for p in pids:
+            ctx.release_palette(p)
+
+
+def test_thread_segmented_full_hd_auto(ctx, oracle):
+    img = synth.gradient_rgb8(1920, 1080, 2)
+    t = sb.Octree(img, 256, False)
+    pid = ctx.palette_from_octree(t)
+    try:
+        want, _, _ = oracle.walk_seq(synth.to_q16(img), 256, False, False)
+        got = ctx.dither_host("seq", img, pid)  # automatic mode: thread walkers for RGB
+        assert np.array_equal(got, want)
+        assert ctx.last_passes >= 1
+    finally:
+        ctx.release_palette(pid)
+
+
+def test_thread_segmented_refuses_alpha_palette(ctx):
+    img = synth.gradient_rgba8(128, 96, 3)
+    t = sb.Octree(img, 16, True)
+    pid = ctx.palette_from_octree(t)
+    try:
+        with pytest.raises(sb.RdbError):
+            ctx.dither_host("seq", img, pid, seq_mode=3)
+    finally:
+        ctx.release_palette(pid)
