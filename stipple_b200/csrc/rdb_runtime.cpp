@@ -834,9 +834,7 @@ int Context::SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStrea
 // until each image's verified prefix covers it.
 int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
   const bool use_cache = o.use_cache != 0;
-  int seg_len = o.seg_len > 0 ? std::max(o.seg_len, 64) : 256;
-  seg_len = (seg_len + 15) & ~15;
-  const int warm_len = std::max(16, o.warm_len > 0 ? o.warm_len : 128);
+  const int warm_len = std::max(16, o.warm_len > 0 ? o.warm_len : 64);
   constexpr int kChunk = 128;
   constexpr int kKeys = 1 << 18;
   std::vector<TswImage> imgs(static_cast<std::size_t>(n));
@@ -845,10 +843,27 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   bool is_float = false;
   int total = 0;
   int64_t positions = 0;
+  int64_t all_px = 0;
+  for (int i = 0; i < n; ++i) {
+    const DevPlan* p = Plan(jobs[i].palette_id);
+    if (p->assoc) return Fail(RDB_E_UNSUPPORTED, "thread segmented walk: alpha-associated palette");
+    plan_max = std::max(plan_max, p->smem);
+    all_px += int64_t{jobs[i].width} * jobs[i].height;
+  }
+  if (TswSmemBytes(plan_max) > smem_optin_) {
+    return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
+  }
+  // Segment length: as given, else the shortest (at least 64) that keeps
+  // every segment of the call on a resident thread -- one wave per pass.
+  int seg_len = o.seg_len;
+  if (seg_len <= 0) {
+    const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_));
+    seg_len = static_cast<int>(std::min<int64_t>(1024, (all_px + resident - 1) / resident));
+  }
+  seg_len = (std::max(seg_len, 64) + 15) & ~15;
   for (int i = 0; i < n; ++i) {
     const rdb_job& j = jobs[i];
     const DevPlan* p = Plan(j.palette_id);
-    if (p->assoc) return Fail(RDB_E_UNSUPPORTED, "thread segmented walk: alpha-associated palette");
     const int32_t* order = nullptr;
     if (int rc = Order(j.width, j.height, s, &order)) return rc;
     TswImage& im = imgs[static_cast<std::size_t>(i)];
@@ -873,11 +888,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     }
     total += im.nsegs;
     positions += (im.n + 15) & ~15;
-    plan_max = std::max(plan_max, p->smem);
     is_float = is_float || j.layout == RDB_RGBAF32;
-  }
-  if (static_cast<std::size_t>(plan_max) > smem_optin_) {
-    return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
   }
   int own_bits = 4;
   while ((1 << own_bits) < 2 * seg_len) ++own_bits;

@@ -113,7 +113,8 @@ __device__ __forceinline__ void red_min(uint32_t* p, uint32_t v) {
 // serially in one lane while the other 31 wait.
 template <bool kFloat>
 __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& im,
-                                            const tw::Plan& P, int k, bool active, int lane) {
+                                            const tw::Plan& P, const double* errp, int k,
+                                            bool active, int lane) {
   const int sid = im.first_seg + k;
   const int begin = k * L.seg_len;
   const int end = active ? min(begin + L.seg_len, im.n) : begin;
@@ -161,6 +162,8 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   double* qe = L.q_end[L.pass & 1] + static_cast<int64_t>(sid) * 64;
   double* qs = L.q_start + static_cast<int64_t>(sid) * 64;
   uint8_t* out = L.chosen + base;
+  const uint8_t* uni = im.uni;
+  uint32_t* usemin = im.usemin;
   const int warp_steps = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(steps));
   int n_own = 0;
   uint32_t acc = 0;
@@ -205,7 +208,7 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
       key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12);
       // A uniform key's search result (and so its memo value) is fixed by the
       // key: no search, no memo, no bookkeeping.
-      const uint8_t uv = __ldg(im.uni + key);
+      const uint8_t uv = __ldg(uni + key);
       const uint32_t gv = keyed ? __ldg(gprev + key) : kNone;  // both loads in flight together
       search = uv == kNotUniform;
       index = uv;
@@ -257,15 +260,14 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
       if (lane == src) index = r;
     }
     if (booked) red_min(gnew + key, (static_cast<uint32_t>(k) << 8) | static_cast<uint32_t>(index));
-    if (from_g) red_min(im.usemin + key, static_cast<uint32_t>(k));
+    if (from_g) red_min(usemin + key, static_cast<uint32_t>(k));
     if (on) {
       if (record) {
         ot[h] = tag | static_cast<uint64_t>(key) | (static_cast<uint64_t>(index) << 24);
         ol[n_own++] = key | (static_cast<uint32_t>(index) << 24);
       }
-      const double* rc = P.rcol<false>(index);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) e[c] = __dadd_rn(static_cast<double>(f[c]), -rc[c]);
+      for (int c = 0; c < 3; ++c) e[c] = __dadd_rn(static_cast<double>(f[c]), -errp[c * kMaxPaletteColors + index]);
       if (live) {
         const int q = (t - begin) & 3;
         acc |= static_cast<uint32_t>(index) << (8 * q);
@@ -307,6 +309,19 @@ __global__ void __launch_bounds__(128, 3) TswWalkKernel(TswLaunch L) {
     for (int i = threadIdx.x; i < im.plan_smem / 16; i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
+  // Residual-side colours channel-planar (colour i of channel c at
+  // c * 256 + i): lanes holding different indices then spread over the banks
+  // instead of meeting in the 32-byte palette rows.
+  double* errp = reinterpret_cast<double*>(smem + L.plan_smem_max);
+  {
+    tw::Plan P0;
+    P0.bind(smem);
+    for (int i = threadIdx.x; i < 3 * kMaxPaletteColors; i += blockDim.x) {
+      const int c = i / kMaxPaletteColors, col = i - c * kMaxPaletteColors;
+      errp[i] = col < P0.h->count ? P0.rcol<false>(col)[c] : 0.0;
+    }
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   // Warps whose segments are all verified or past the image leave together.
   const int warp_k0 = ch.k0 + static_cast<int>(threadIdx.x & ~31u);
@@ -316,7 +331,7 @@ __global__ void __launch_bounds__(128, 3) TswWalkKernel(TswLaunch L) {
   const bool active = static_cast<int>(threadIdx.x) < ch.count && k >= front;
   tw::Plan P;
   P.bind(smem);
-  WalkSegment<kFloat>(L, im, P, active ? k : warp_end - 1, active, lane);
+  WalkSegment<kFloat>(L, im, P, errp, active ? k : warp_end - 1, active, lane);
 }
 
 // G_new = the entries of G_prev that verified segments made; usemin cleared.
@@ -405,7 +420,23 @@ __global__ void TswScatter(TswLaunch L, int64_t total) {
 
 }  // namespace
 
-std::size_t TswSmemBytes(int plan_smem_max) { return static_cast<std::size_t>(plan_smem_max); }
+std::size_t TswSmemBytes(int plan_smem_max) {
+  return static_cast<std::size_t>(plan_smem_max) + 3 * kMaxPaletteColors * sizeof(double);
+}
+
+int TswResidentThreads(int plan_smem_max, int sm_count) {
+  const int smem = static_cast<int>(TswSmemBytes(plan_smem_max));
+  if (cudaFuncSetAttribute(TswWalkKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+      cudaSuccess) {
+    return 0;
+  }
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, TswWalkKernel<false>, 128, smem) !=
+      cudaSuccess) {
+    return 0;
+  }
+  return blocks * 128 * sm_count;
+}
 
 cudaError_t LaunchTswGather(const TswLaunch& L, int64_t total, cudaStream_t s) {
   if (total <= 0) return cudaSuccess;

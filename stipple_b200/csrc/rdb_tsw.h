@@ -94,6 +94,8 @@ struct TswLaunch {
 };
 
 std::size_t TswSmemBytes(int plan_smem_max);
+// Walker threads the device holds at once (0 if the query fails).
+int TswResidentThreads(int plan_smem_max, int sm_count);
 // Samples of every image in visit order, into L.cx.
 cudaError_t LaunchTswGather(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
 // G_new = verified entries of G_prev, usemin cleared (memo only).
