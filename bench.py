@@ -185,6 +185,7 @@ def run_ours(a, rank: int, world: int):
     if world > 1:
         torch.distributed.barrier()
     times = []
+    ctx.profile(True)  # walk-kernel events on the launching stream, launch counts
     with ClockSampler(dev) as clk:
         for _ in range(a.steps):
             flush.fill_(1)
@@ -196,6 +197,8 @@ def run_ours(a, rank: int, world: int):
             ctx.synchronize(s)
             times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
+    kstats = ctx.stats()
+    ctx.profile(False)
     total_ms = sum(times)
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
@@ -219,16 +222,29 @@ def run_ours(a, rank: int, world: int):
            "h2d_bytes_per_step": int(img.nbytes), "d2h_bytes_per_step": int(W * H)}
 
     hbm, peak_kind = peaks()
-    alg_bytes = px * 4  # 3 B of RGB8 read + 1 B of index written per pixel
-    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    # Dominant kernel: the segment walk (TswWalkKernel), timed per launch with
+    # CUDA events on its stream inside the library.  Algorithmic bytes per
+    # walked position: the packed sample (4 B), its uniform-key byte (1 B), its
+    # first-touch word (4 B) and the index written (1 B).
+    launches = max(1, kstats["walk_launches"])
+    walk_ms = kstats["walk_ms"] / launches
+    pos_per_launch = kstats["walk_positions"] / launches
+    achieved = pos_per_launch * 10 / (walk_ms / 1e3) / 1e9 if walk_ms > 0 else 0.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                "kernel": "SeqWalkKernel",
-                "note": "the sequential walk is a dependent chain: its real bound is "
-                        "the per-pixel chain latency, see chain"}
-    chain = {"ns_per_px": ms_step * 1e6 / px, "clock_mhz": clk.summary()["sm_mhz"]}
-    if chain["clock_mhz"]:
-        chain["cycles_per_px"] = chain["ns_per_px"] * chain["clock_mhz"] / 1e3
+                "kernel": "TswWalkKernel", "walk_ms_per_launch": walk_ms,
+                "positions_per_launch": pos_per_launch,
+                "note": "each segment is a dependent chain walked by one thread: the kernel "
+                        "is bound by the per-step chain latency, not HBM (see chain); DRAM "
+                        "traffic per launch is in profiles/"}
+    clock = clk.summary()["sm_mhz"]
+    seg = int(kstats["seg_len"])
+    chain = {"passes_per_step": kstats["passes"] / max(1, a.steps), "ns_per_px": ms_step * 1e6 / px,
+             "walk_share": kstats["walk_ms"] / total_ms if total_ms else None,
+             "segment_len": seg, "concurrent_chains": int(kstats["chains"]), "clock_mhz": clock}
+    if clock and walk_ms > 0 and seg:
+        # A launch walks every unverified segment once: seg steps per chain.
+        chain["cycles_per_chain_step"] = walk_ms * 1e-3 * clock * 1e6 / seg
 
     out = {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
@@ -240,7 +256,7 @@ def run_ours(a, rank: int, world: int):
                       "l2": "flushed between timed steps (256 MB write)",
                       "parallelism": f"replicas x{world}"},
            "e2e": e2e, "roofline": roofline, "chain": chain, "clocks": clk.summary(),
-           "gpu_launches": a.steps}
+           "gpu_launches": int(kstats["launches"])}
 
     if rank == 0 and not a.skip_extra:
         out["blocks"] = bench_blocks(ctx, s, a, tree, pid, hbm)

@@ -88,6 +88,22 @@ size_t rdb_context_bytes(const rdb_context* ctx);
  * reference counterpart: the reference walks one chain. */
 int rdb_context_last_passes(const rdb_context* ctx);
 
+/* Device-side counters of the segmented sequential walk, kept while profiling
+ * is on (rdb_context_profile(ctx, 1) clears them).  Walk-kernel times are CUDA
+ * events recorded on the launching stream around each walk launch.  No
+ * reference counterpart. */
+typedef struct rdb_kernel_stats {
+  int64_t walk_launches;   /* segment-walk kernel launches */
+  double walk_ms;          /* their summed device time */
+  int64_t walk_positions;  /* positions those launches walked, warm-ups included */
+  int64_t passes;          /* segmented-walk passes */
+  int64_t launches;        /* kernels the context launched for the sequential engine */
+  int64_t seg_len;         /* segment length of the last segmented walk */
+  int64_t chains;          /* segments (concurrent chains) of the last segmented walk */
+} rdb_kernel_stats;
+int rdb_context_profile(rdb_context* ctx, int enable);
+int rdb_context_stats(const rdb_context* ctx, rdb_kernel_stats* out);
+
 /* A palette and its colour tree, in the reference's own terms
  * (rd::Palette, include/rd_riemersma.h:63-67; rd::QNode, include/rd_octree.h:43-52). */
 typedef struct rdb_palette_desc {

@@ -31,6 +31,13 @@ class RdbError(RuntimeError):
         self.code = code
 
 
+class KernelStats(C.Structure):
+    """rdb_kernel_stats (include/rdb.h)."""
+    _fields_ = [("walk_launches", C.c_int64), ("walk_ms", C.c_double),
+                ("walk_positions", C.c_int64), ("passes", C.c_int64), ("launches", C.c_int64),
+                ("seg_len", C.c_int64), ("chains", C.c_int64)]
+
+
 class Options(C.Structure):
     _fields_ = [
         ("diffusion", C.c_double),
@@ -99,6 +106,8 @@ SIGNATURES = {
     "rdb_context_destroy": (None, [C.c_void_p]),
     "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
     "rdb_context_last_passes": (C.c_int, [C.c_void_p]),
+    "rdb_context_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "rdb_context_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rdb_palette_create": (C.c_int, [C.c_void_p, C.POINTER(PaletteDesc), C.POINTER(C.c_int)]),
     "rdb_palette_from_octree": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "rdb_plan_build": (C.c_int, [C.POINTER(PaletteDesc), C.c_void_p, C.c_size_t,
@@ -241,6 +250,15 @@ class Context:
     def last_passes(self) -> int:
         """Passes the last segmented sequential walk took."""
         return load().rdb_context_last_passes(self.handle)
+
+    def profile(self, enable: bool = True) -> None:
+        """Turns the walk-kernel counters on or off (and clears them)."""
+        _check(load().rdb_context_profile(self.handle, int(enable)))
+
+    def stats(self) -> dict:
+        st = KernelStats()
+        _check(load().rdb_context_stats(self.handle, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in KernelStats._fields_}
 
     # -- palettes ---------------------------------------------------------
     def palette_from_octree(self, tree: Octree) -> int:

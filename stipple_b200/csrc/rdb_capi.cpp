@@ -154,6 +154,17 @@ size_t rdb_context_bytes(const rdb_context* ctx) { return ctx ? ctx->impl.bytes(
 
 int rdb_context_last_passes(const rdb_context* ctx) { return ctx ? ctx->impl.last_passes() : 0; }
 
+int rdb_context_profile(rdb_context* ctx, int enable) {
+  if (!ctx) return Guard("rdb_context_profile");
+  return ctx->impl.Profile(enable != 0);
+}
+
+int rdb_context_stats(const rdb_context* ctx, rdb_kernel_stats* out) {
+  if (!ctx || !out) return Guard("rdb_context_stats");
+  *out = ctx->impl.stats();
+  return RDB_OK;
+}
+
 int rdb_palette_create(rdb_context* ctx, const rdb_palette_desc* d, int* palette_id) {
   if (!ctx || !d || !palette_id || !d->colors || !d->child || !d->color_number ||
       !d->number_unique) {

@@ -55,7 +55,23 @@ Context::~Context() {
                     &tsw_count_, &tsw_cx_, &tsw_chosen_, &tsw_g_}) {
     Release(b);
   }
+  for (cudaEvent_t& ev : ev_) {
+    if (ev) cudaEventDestroy(ev);
+  }
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Context::Profile(bool on) {
+  cudaSetDevice(device_);
+  for (cudaEvent_t& ev : ev_) {
+    if (!ev) {
+      const cudaError_t e = cudaEventCreate(&ev);
+      if (e != cudaSuccess) return CudaFail(e, "profiling events");
+    }
+  }
+  profiling_ = on;
+  stats_ = rdb_kernel_stats{};
+  return RDB_OK;
 }
 
 int Context::Init(int device, std::size_t budget) {
@@ -971,7 +987,9 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     int* cur = L.bad[pass & 1];
     cudaMemsetAsync(cur, 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
     if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
+    if (profiling_) cudaEventRecord(ev_[0], s);
     if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
+    if (profiling_) cudaEventRecord(ev_[1], s);
     if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
     if ((e = cudaMemcpyAsync(bad_h.data(), cur, static_cast<std::size_t>(n) * sizeof(int),
                              cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
@@ -983,6 +1001,25 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     if (status != 0) {
       cudaMemset(status_.ptr, 0, sizeof(int));
       return Fail(RDB_E_DEVICE, "segmented walk reported status " + std::to_string(status));
+    }
+    if (profiling_) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+      stats_.walk_ms += ms;
+      stats_.walk_launches += 1;
+      stats_.passes += 1;
+      stats_.launches += 1 + 1 + (use_cache ? 2 : 0);  // walk, segment check, [prepare, key check]
+      for (int i = 0; i < n; ++i) {
+        const TswImage& im = imgs[static_cast<std::size_t>(i)];
+        const int f0 = std::max(front[static_cast<std::size_t>(i)], 0);
+        if (f0 >= im.nsegs) continue;
+        stats_.walk_positions += im.n - static_cast<int64_t>(f0) * seg_len;
+        if (pass == 0) {
+          for (int k = std::max(f0, 1); k < im.nsegs; ++k) {
+            stats_.walk_positions += std::min(k * seg_len, warm_len);
+          }
+        }
+      }
     }
     // The verified prefix of every unfinished image grows by at least one
     // segment a pass (its first walked segment started from exact state);
@@ -1001,6 +1038,11 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   }
   last_passes_ = pass + 1;
   if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
+  if (profiling_) {
+    stats_.launches += 2;  // gather, scatter
+    stats_.seg_len = seg_len;
+    stats_.chains = total;
+  }
   return RDB_OK;
 }
 

@@ -127,9 +127,14 @@ class Context {
   DevBuf tsw_chosen_;
   DevBuf tsw_g_;
   int last_passes_ = 0;
+  bool profiling_ = false;
+  rdb_kernel_stats stats_{};
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
 
  public:
   int last_passes() const { return last_passes_; }
+  int Profile(bool on);
+  const rdb_kernel_stats& stats() const { return stats_; }
 };
 
 }  // namespace rdb
