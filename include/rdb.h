@@ -49,6 +49,12 @@ int rdb_device_name(int device, char* buf, size_t len);
 /* Replaces CudaAllocPinned / CudaFreePinned (include/rd_riemersma.h:480-481). */
 void* rdb_alloc_pinned(size_t bytes);
 void rdb_free_pinned(void* p);
+/* Whole frames of width x height that one host-buffer call of `engine` can
+ * hold on `device` within min(free memory, vram_budget) (budget 0 = free
+ * memory): staging plus the engine's scratch per frame, after the fixed
+ * per-call tables; at most 4096.  Replaces CudaMaxFrames
+ * (include/rd_riemersma.h:288), which sizes the reference's own buffers. */
+int rdb_max_frames(int device, int engine, size_t width, size_t height, size_t vram_budget);
 
 /* ---- palette building -----------------------------------------------------
  * Replaces rd::ColorTree::Build (include/rd_octree.h:62-63): ImageMagick's

@@ -192,6 +192,37 @@ class Oracle:
         n = self.lib.orc_seq_order(w, h, out)
         return out[:n]
 
+    def walk_seq_frame(self, tree_src: np.ndarray, frame: np.ndarray, max_colors: int,
+                       assoc: bool, gray: bool, diffusion: float = 1.0,
+                       use_cache: bool = True) -> np.ndarray:
+        """RiemersmaWalkCpu of `frame` with the tree built from `tree_src`."""
+        h, w = tree_src.shape[:2]
+        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            out = np.ascontiguousarray(frame, dtype=np.float32).reshape(-1).copy()
+            self.lib.ref_walk_seq(t, float(diffusion), int(use_cache), w, h, out)
+            return out.reshape(h, w, 4)
+        finally:
+            self.lib.ref_tree_free(t)
+
+    def walk_blocks_frames(self, tree_src: np.ndarray, frames: np.ndarray, max_colors: int,
+                           assoc: bool, gray: bool, block: int, diffusion: float = 1.0):
+        """RiemersmaBlocksCpu over F frames in place ((F, H, W, 4) float32), the
+        tree built from `tree_src`.  Returns (0, "") or (-1, refusal)."""
+        h, w = tree_src.shape[:2]
+        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            flat = frames.reshape(-1)
+            assert flat.base is frames or flat.base is frames.base or np.shares_memory(flat, frames)
+            err = C.create_string_buffer(1024)
+            rc = self.lib.ref_walk_blocks(t, float(diffusion), int(block), w, h, flat,
+                                          frames.shape[0], err, 1024)
+            return rc, err.value.decode()
+        finally:
+            self.lib.ref_tree_free(t)
+
     def block_order(self, w: int, h: int):
         out = np.empty(w * h + 1, np.int32)
         owner = np.empty(max(w * h, 1), np.int32)
@@ -299,6 +330,37 @@ class RefLib:
         finally:
             self.lib.ref_tree_free(t)
 
+    def walk_seq_frame(self, tree_src: np.ndarray, frame: np.ndarray, max_colors: int,
+                       assoc: bool, gray: bool, diffusion: float = 1.0,
+                       use_cache: bool = True) -> np.ndarray:
+        """RiemersmaWalkCpu of `frame` with the tree built from `tree_src`."""
+        h, w = tree_src.shape[:2]
+        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            out = np.ascontiguousarray(frame, dtype=np.float32).reshape(-1).copy()
+            self.lib.ref_walk_seq(t, float(diffusion), int(use_cache), w, h, out)
+            return out.reshape(h, w, 4)
+        finally:
+            self.lib.ref_tree_free(t)
+
+    def walk_blocks_frames(self, tree_src: np.ndarray, frames: np.ndarray, max_colors: int,
+                           assoc: bool, gray: bool, block: int, diffusion: float = 1.0):
+        """RiemersmaBlocksCpu over F frames in place ((F, H, W, 4) float32), the
+        tree built from `tree_src`.  Returns (0, "") or (-1, refusal)."""
+        h, w = tree_src.shape[:2]
+        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), int(gray))
+        try:
+            flat = frames.reshape(-1)
+            assert flat.base is frames or flat.base is frames.base or np.shares_memory(flat, frames)
+            err = C.create_string_buffer(1024)
+            rc = self.lib.ref_walk_blocks(t, float(diffusion), int(block), w, h, flat,
+                                          frames.shape[0], err, 1024)
+            return rc, err.value.decode()
+        finally:
+            self.lib.ref_tree_free(t)
+
     def block_order(self, w: int, h: int):
         out = np.empty(w * h + 1, np.int32)
         owner = np.empty(max(w * h, 1), np.int32)
@@ -315,6 +377,60 @@ class RefLib:
         w = np.zeros(16, np.float64)
         self.lib.ref_error_weights(w)
         return w
+
+
+DROPIN_SO = os.path.join(HERE, "_ref", "librddropin.so")
+
+
+class DropinLib:
+    """The reference-facing C++ layer (stipple_b200/dropin) driven through
+    oracle/dropin_shim.cpp with trees from the reference's ColorTree::Build.
+    Test infrastructure: present only where the reference headers were."""
+
+    ENGINES = {"walk": 0, "blocks": 1, "approx": 2, "plugin": 3}
+
+    def __init__(self, path: str = DROPIN_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = lib = C.CDLL(path)
+        lib.dropin_available.restype = C.c_int
+        lib.dropin_max_frames.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t]
+        lib.dropin_max_frames.restype = C.c_int
+        lib.dropin_inverse_filter.argtypes = [C.c_int, C.c_double,
+                                              np.ctypeslib.ndpointer(np.float64)]
+        lib.dropin_inverse_filter.restype = C.c_int
+        lib.dropin_alloc_pinned.argtypes = [C.c_size_t]
+        lib.dropin_alloc_pinned.restype = C.c_void_p
+        lib.dropin_free_pinned.argtypes = [C.c_void_p]
+        f32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        lib.dropin_run.argtypes = [C.c_int, f32, C.c_size_t, C.c_size_t, C.c_int, C.c_int, C.c_int,
+                                   f32, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_int, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
+        lib.dropin_run.restype = C.c_int
+
+    def run(self, engine: str, tree_src: np.ndarray, frames: np.ndarray, colors: int,
+            assoc: bool = False, gray: bool = False, diffusion: float = 1.0,
+            use_cache: bool = True, block: int = 512, iterations: int = 20, taps: int = 96,
+            slot: int = 0):
+        """Dithers `frames` ((F, H, W, 4) float32, Q16) in place; returns
+        (error or "", device name)."""
+        h, w = tree_src.shape[:2]
+        err = C.create_string_buffer(512)
+        dev = C.create_string_buffer(256)
+        src = np.ascontiguousarray(tree_src, np.float32)
+        rc = self.lib.dropin_run(self.ENGINES[engine], src, w, h, colors, int(assoc), int(gray),
+                                 frames, frames.shape[0], float(diffusion), int(use_cache), block,
+                                 iterations, taps, slot, err, 512, dev, 256)
+        return ("" if rc == 0 else err.value.decode()), dev.value.decode()
+
+    def inverse_filter(self, taps: int, diffusion: float = 1.0) -> np.ndarray:
+        out = np.zeros(taps + 1, np.float64)
+        n = self.lib.dropin_inverse_filter(taps, diffusion, out)
+        return out[:n]
+
+
+def dropin_available() -> bool:
+    return os.path.exists(DROPIN_SO)
 
 
 def ref_available() -> bool:

@@ -106,6 +106,7 @@ SIGNATURES = {
     "rdb_context_destroy": (None, [C.c_void_p]),
     "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
     "rdb_context_last_passes": (C.c_int, [C.c_void_p]),
+    "rdb_max_frames": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t]),
     "rdb_context_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "rdb_context_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rdb_palette_create": (C.c_int, [C.c_void_p, C.POINTER(PaletteDesc), C.POINTER(C.c_int)]),

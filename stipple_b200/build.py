@@ -84,8 +84,43 @@ def _lib_current() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 
+# The reference-facing C++ layer (stipple_b200/dropin) is compiled against
+# the reference's own headers, where that tree is present; elsewhere the
+# libraries built here earlier are used as they are.
+REFERENCE = os.environ.get("RDB_REFERENCE", "/root/reference")
+DROPIN = os.path.join(HERE, "dropin")
+DROPIN_LIB = os.path.join(LIBDIR, "librd_b200_dropin.so")
+PLUGIN_LIB = os.path.join(LIBDIR, "librd_b200_plugin.so")
+
+
+def build_dropin() -> bool:
+    """Builds librd_b200_dropin.so (the seven engine symbols of
+    rd_riemersma.h) and librd_b200_plugin.so (the "riemersma-b200" registry
+    entry).  Returns False when the reference headers are absent."""
+    inc = os.path.join(REFERENCE, "include")
+    if not os.path.isdir(inc):
+        return False
+    common = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-I", inc,
+              "-I", os.path.join(ROOT, "include"), "-Wl,-rpath,$ORIGIN"]
+    steps = [
+        (DROPIN_LIB, [os.path.join(DROPIN, "rd_b200_dropin.cpp")],
+         ["-L", LIBDIR, "-lrdb_b200"]),
+        (PLUGIN_LIB, [os.path.join(DROPIN, "rd_b200_plugin.cpp")],
+         ["-L", LIBDIR, "-lrd_b200_dropin"]),
+    ]
+    for out, srcs, libs in steps:
+        if os.path.exists(out) and all(os.path.getmtime(x) <= os.path.getmtime(out)
+                                       for x in srcs + [LIB]):
+            continue
+        r = subprocess.run(common + ["-o", out] + srcs + libs, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"drop-in build failed ({out}):\n{r.stdout}\n{r.stderr}")
+    return True
+
+
 def build(ptxas_verbose: bool = False, force: bool = False) -> str:
     if not force and not ptxas_verbose and _lib_current():
+        build_dropin()
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
@@ -103,6 +138,7 @@ def build(ptxas_verbose: bool = False, force: bool = False) -> str:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     if logs and ptxas_verbose:
         print("\n".join(logs))
+    build_dropin()
     return LIB
 
 

@@ -69,6 +69,34 @@ void rdb_free_pinned(void* p) {
   if (p) cudaFreeHost(p);
 }
 
+int rdb_max_frames(int device, int engine, size_t width, size_t height, size_t vram_budget) {
+  if (width == 0 || height == 0) return 0;
+  if (cudaSetDevice(device) != cudaSuccess) return 0;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+  if (vram_budget != 0 && vram_budget < free_b) free_b = vram_budget;
+  const size_t px = width * height;
+  // Fixed per call: the visit order (4 B per position), the palette plan and
+  // uniform-key table, the status and work words.
+  const size_t fixed = 4 * px + (size_t{1} << 20);
+  // Per frame: RgbaF staging in and out (16 + 16 B), the index map (1 B), and
+  // the engine's scratch: the segmented walk's gathered samples, chosen
+  // indices, memo tables and queues (~60 B) plus its 3 MB of key maps; the
+  // block and Jacobi engines' curve-ordered copies (~20 B).
+  size_t per_px = 33, per_frame_fixed = 0;
+  if (engine == RDB_ENGINE_SEQ) {
+    per_px += 60;
+    per_frame_fixed = size_t{3} << 20;
+  } else {
+    per_px += 20;
+  }
+  const size_t per_frame = per_px * px + per_frame_fixed;
+  if (free_b < fixed + per_frame) return 0;
+  size_t frames = (free_b - fixed) / per_frame;
+  if (frames > 4096) frames = 4096;
+  return static_cast<int>(frames);
+}
+
 int rdb_octree_build(const void* pixels, int layout, size_t width, size_t height,
                      size_t row_stride, int max_colors, int associate_alpha, int grayscale,
                      rdb_octree** out) {

@@ -815,6 +815,7 @@ int Context::SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cuda
     }
   }
   last_passes_ = pass;
+  if ((e = LaunchSswRgba(L, n, s)) != cudaSuccess) return CudaFail(e, "RgbaF output");
   return RDB_OK;
 }
 

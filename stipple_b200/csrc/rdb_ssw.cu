@@ -317,11 +317,6 @@ __device__ void SegWalk(const SswLaunch& L, const SswImage& im, const SswSeg& sg
         const int rs = ring_slot(q);
         const int o = ring_ord[rs];
         im.indices[o] = static_cast<uint8_t>(my_index);
-        if (im.rgba_out) {
-          const float4 pc = reinterpret_cast<const float4*>(im.plan + P.h->off_out)[my_index];
-          const float a = kAssoc ? pc.w : ring_pix[rs].w;
-          im.rgba_out[o] = make_float4(pc.x, pc.y, pc.z, a);
-        }
       }
       __syncwarp();
     }
@@ -440,6 +435,23 @@ __global__ void SswVerifyKernel(SswLaunch L) {
   if (!all && lane == 0) atomicMin(&L.first_bad[sg.image], sg.k);
 }
 
+// RgbaF output from the final indices, once every segment is verified: the
+// walk itself never writes it, since RgbaF input is dithered in place and a
+// later pass may still read the source pixels.
+__global__ void SswRgbaKernel(SswLaunch L, int n_images) {
+  const int m = blockIdx.y;
+  if (m >= n_images) return;
+  const SswImage& im = L.images[m];
+  if (!im.rgba_out) return;
+  const PlanHeader* h = reinterpret_cast<const PlanHeader*>(im.plan);
+  const float4* pal = reinterpret_cast<const float4*>(im.plan + h->off_out);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < im.n; p += gridDim.x * blockDim.x) {
+    const float4 pc = pal[im.indices[p]];
+    const float a = im.assoc ? pc.w : load_sample(im.pixels, im.layout, im.row_stride, im.width, p).w;
+    im.rgba_out[p] = make_float4(pc.x, pc.y, pc.z, a);
+  }
+}
+
 __global__ void SswCarryKernel(SswLaunch L) {
   const int w = blockIdx.x;
   if (w >= L.n_work) return;
@@ -479,6 +491,12 @@ cudaError_t LaunchSswBuildG(const SswLaunch& L, int total_segs, cudaStream_t s) 
 cudaError_t LaunchSswVerify(const SswLaunch& L, cudaStream_t s) {
   if (L.n_work <= 0) return cudaSuccess;
   SswVerifyKernel<<<(L.n_work + 7) / 8, 256, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchSswRgba(const SswLaunch& L, int n_images, cudaStream_t s) {
+  if (n_images <= 0) return cudaSuccess;
+  SswRgbaKernel<<<dim3(64, n_images), 256, 0, s>>>(L, n_images);
   return cudaGetLastError();
 }
 

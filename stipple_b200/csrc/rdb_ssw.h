@@ -88,6 +88,8 @@ cudaError_t LaunchSswWalk(const SswLaunch& L, int grid, cudaStream_t s);
 cudaError_t LaunchSswBuildG(const SswLaunch& L, int total_segs, cudaStream_t s);
 // Checks the active segments; records the first failing segment per image.
 cudaError_t LaunchSswVerify(const SswLaunch& L, cudaStream_t s);
+// RgbaF output of every image with one, from its final indices.
+cudaError_t LaunchSswRgba(const SswLaunch& L, int n_images, cudaStream_t s);
 // q_start[k] = q_end[k-1] for the active segments with k > 0.
 cudaError_t LaunchSswCarry(const SswLaunch& L, cudaStream_t s);
 std::size_t SswSmemBytes(int plan_smem_max, int cache_bits);

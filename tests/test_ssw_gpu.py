@@ -82,3 +82,23 @@ def test_segmented_full_hd(ctx, oracle):
         assert np.array_equal(auto, want)
     finally:
         ctx.release_palette(pid)
+
+
+def test_segmented_float_in_place(ctx, oracle):
+    """RgbaF input is dithered in place on the device: later passes must still
+    see the source pixels, so the RgbaF result is written once, at the end."""
+    for alpha in (True, False):
+        img = synth.gradient_rgba8(192, 160, 31) if alpha else synth.gradient_rgb8(192, 160, 31)
+        q = synth.to_q16(img)
+        t = sb.Octree(img, 64, alpha)
+        pid = ctx.palette_from_octree(t)
+        try:
+            for mode in ((2, 3) if not alpha else (2,)):
+                idx, rgba = ctx.dither_host("seq", q, pid, rgba=True, seq_mode=mode, seg_len=128,
+                                            warm_len=32)
+                want, out, _ = oracle.walk_seq(q, 64, alpha, t.grayscale)
+                assert np.array_equal(idx, want), (alpha, mode)
+                ch = 4 if alpha else 3
+                assert np.array_equal(rgba[..., :ch].view(np.uint32), out[..., :ch].view(np.uint32))
+        finally:
+            ctx.release_palette(pid)
