@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--block-frames", type=int, default=16)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--skip-extra", action="store_true")
+    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "blocks"],
+                    help="run only that workload's device steps (for ncu captures) and print "
+                         "its timing; no JSON contract line")
     return ap.parse_args()
 
 
@@ -362,8 +365,52 @@ def run_reference(a):
                     "d2h_bytes_per_step": 0}}
 
 
+def profile_case(a):
+    """The device steps of one workload and nothing else: the command the
+    ncu summaries under profiles/ were taken with."""
+    import torch
+    import stipple_b200 as sb
+    from stipple_b200 import synth
+    torch.cuda.set_device(0)
+    ctx = sb.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    s = stream.cuda_stream
+    W, H, C = HEADLINE["width"], HEADLINE["height"], HEADLINE["colors"]
+    img = synth.gradient_rgb8(W, H, HEADLINE["seed"])
+    pid = ctx.palette_from_octree(sb.Octree(img, C, False, False))
+    if a.profile_case == "seq":
+        d = torch.from_numpy(img).cuda()
+        o = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+        jobs = [dict(pixels=d.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
+                     indices=o.data_ptr())]
+        opts = {}
+    else:
+        n = a.block_frames
+        frames = [torch.from_numpy(synth.video_frame(W, H, 3, f)).cuda() for f in range(n)]
+        outs = [torch.empty((H, W), dtype=torch.uint8, device="cuda") for _ in range(n)]
+        jobs = [dict(pixels=f.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
+                     indices=x.data_ptr()) for f, x in zip(frames, outs)]
+        opts = {"block": 256}
+    engine = "seq" if a.profile_case == "seq" else "blocks"
+    for _ in range(a.warmup):
+        ctx.dither(engine, jobs, stream=s, **opts)
+    ctx.synchronize(s)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        ctx.dither(engine, jobs, stream=s, **opts)
+    e1.record(stream)
+    ctx.synchronize(s)
+    print(f"{a.profile_case}: {e0.elapsed_time(e1) / max(1, a.steps):.3f} ms per step", flush=True)
+
+
 def main():
     a = parse()
+    if a.profile_case != "none":
+        profile_case(a)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if a.impl == "reference":

@@ -75,13 +75,18 @@ def test_seq_diffusion_and_cache_options(ctx, oracle):
                 idx = ctx.dither_host("seq", img, pid, diffusion=diff, use_cache=cache)
                 oidx, _, _ = oracle.walk_seq(q, 32, False, False, diffusion=diff, use_cache=bool(cache))
                 assert np.array_equal(idx, oidx), (diff, cache)
+        # The one-warp chain's shared-memory memo cache (the automatic mode
+        # segments an image this size, which has no such cache).
+        for mode in (0, 1):
+            idx = ctx.dither_host("seq", img, pid, seq_mode=mode)
+            assert np.array_equal(idx, oracle.walk_seq(q, 32, False, False)[0]), mode
         for bits in (4, 8, 12, 15):
-            idx = ctx.dither_host("seq", img, pid, cache_bits=bits)
+            idx = ctx.dither_host("seq", img, pid, cache_bits=bits, seq_mode=1)
             oidx, _, _ = oracle.walk_seq(q, 32, False, False)
             assert np.array_equal(idx, oidx), bits
         # 2^17 entries do not fit in shared memory: refused, not truncated.
         with pytest.raises(sb.RdbError):
-            ctx.dither_host("seq", img, pid, cache_bits=17)
+            ctx.dither_host("seq", img, pid, cache_bits=17, seq_mode=1)
     finally:
         ctx.release_palette(pid)
 
@@ -125,7 +130,7 @@ def test_seq_batch_equals_solo(ctx, oracle):
         for k in range(len(imgs)):
             assert np.array_equal(again[k], want[k])
         with pytest.raises(sb.RdbError):
-            ctx.dither_host("seq", imgs[0], pids[0], cache_bits=3)
+            ctx.dither_host("seq", imgs[0], pids[0], cache_bits=3, seq_mode=1)
     finally:
         for p in pids:
             ctx.release_palette(p)
