@@ -233,8 +233,11 @@ def run_ours(a, rank: int, world: int):
     walk_ms = kstats["walk_ms"] / launches
     pos_per_launch = kstats["walk_positions"] / launches
     achieved = pos_per_launch * 10 / (walk_ms / 1e3) / 1e9 if walk_ms > 0 else 0.0
+    # DRAM bytes of one walk launch of this workload from ncu (dram__bytes_read
+    # + dram__bytes_write, pass 31), profiles/tsw_walk_4k_rgb8_256c.md.
+    traffic = 63954432 + 5931776
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "TswWalkKernel", "walk_ms_per_launch": walk_ms,
                 "positions_per_launch": pos_per_launch,
                 "note": "each segment is a dependent chain walked by one thread: the kernel "
