@@ -132,6 +132,9 @@ int rdb_palette_create(rdb_context* ctx, const rdb_palette_desc* desc, int* pale
  * most `cap` bytes and the full size to *size. */
 int rdb_plan_build(const rdb_palette_desc* desc, void* out, size_t cap, size_t* size);
 int rdb_palette_from_octree(rdb_context* ctx, const rdb_octree* t, int* palette_id);
+/* Every stream other than the context's own on which the palette was used
+ * must be synchronised first (the context's stream is drained here); the
+ * palette's device blocks return to the context's pool. */
 int rdb_palette_destroy(rdb_context* ctx, int palette_id);
 /* The palette's uniform-key table (stipple_b200/csrc/rdb_uniform.h) copied to
  * host memory: 2^18 bytes, one per 6-bit-per-channel memo key, holding the
@@ -209,6 +212,72 @@ typedef struct rdb_host_job {
 
 int rdb_dither_host(rdb_context* ctx, int engine, const rdb_host_job* jobs, int n_jobs,
                     const rdb_options* opts);
+
+/* ---- serving ----------------------------------------------------------------
+ * A request loop over one device: requests of mixed sizes, palettes and
+ * engines are submitted from any thread; host threads build each request's
+ * palette (the library's octree, rdb_octree_build); requests are admitted
+ * while the device-memory estimate of everything in flight stays within
+ * `memory_budget`; idle device workers (each its own context and stream)
+ * take every admitted request of one engine and one option set as one batch,
+ * so requests that arrive while others are on the device join the next
+ * batch and batches on different workers overlap.  Results are bit-identical
+ * to the same request alone.  No reference counterpart: rdither dithers one
+ * job per call. */
+typedef struct rdb_server rdb_server;
+
+typedef struct rdb_server_options {
+  int device;
+  size_t memory_budget;   /* admission cap in bytes (0 = 90 % of free memory) */
+  int workers;            /* device workers (0 = 4) */
+  int max_batch;          /* requests per batch (0 = 512) */
+  int host_threads;       /* palette builders (0 = hardware threads) */
+} rdb_server_options;
+
+typedef struct rdb_request {
+  const void* pixels;     /* host, row-major, `layout`; must stay valid until completion */
+  size_t row_stride;      /* bytes (0 = packed) */
+  int width;
+  int height;
+  int layout;
+  int colors;             /* palette size requested from the octree */
+  int associate_alpha;    /* palette associates alpha (RGBA input only) */
+  int engine;             /* RDB_ENGINE_* */
+  rdb_options options;
+  uint8_t* indices;       /* host, width*height */
+  float* rgba_out;        /* optional host RgbaF result */
+} rdb_request;
+
+typedef struct rdb_request_result {
+  int status;             /* RDB_OK or the failing call's code */
+  double queue_ms;        /* submit -> palette built */
+  double admit_ms;        /* palette built -> on the device */
+  double device_ms;       /* batch call (uploads, walk, downloads) */
+  double total_ms;        /* submit -> result in host memory */
+  int batch_size;         /* requests in its batch */
+} rdb_request_result;
+
+typedef struct rdb_server_stats {
+  int64_t completed;
+  int64_t failed;
+  int64_t pixels;
+  int64_t batches;
+  double p50_ms;          /* total latency percentiles over completed requests */
+  double p99_ms;
+  double max_ms;
+  double mpx_per_s;       /* pixels / (last completion - first submission) */
+  size_t peak_admitted_bytes;
+} rdb_server_stats;
+
+int rdb_server_create(const rdb_server_options* opts, rdb_server** out);
+/* Non-blocking; the request (and its buffers) must outlive its completion. */
+int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0 = forever) for one request; RDB_E_TIMEOUT when
+ * it is not done yet.  The ticket is released once waited for successfully. */
+int rdb_server_wait(rdb_server* s, uint64_t ticket, int timeout_ms, rdb_request_result* out);
+int rdb_server_stats_get(rdb_server* s, rdb_server_stats* out);
+/* Finishes everything submitted, then stops the threads. */
+void rdb_server_destroy(rdb_server* s);
 
 /* Sequential-exact walk of one image without allocating any device memory.
  * This entry point has no counterpart in the reference.

@@ -55,6 +55,32 @@ class Options(C.Structure):
     ]
 
 
+class ServerOptions(C.Structure):
+    """rdb_server_options (include/rdb.h)."""
+    _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t), ("workers", C.c_int),
+                ("max_batch", C.c_int), ("host_threads", C.c_int)]
+
+
+class Request(C.Structure):
+    """rdb_request (include/rdb.h)."""
+    _fields_ = [("pixels", C.c_void_p), ("row_stride", C.c_size_t), ("width", C.c_int),
+                ("height", C.c_int), ("layout", C.c_int), ("colors", C.c_int),
+                ("associate_alpha", C.c_int), ("engine", C.c_int), ("options", Options),
+                ("indices", C.c_void_p), ("rgba_out", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("queue_ms", C.c_double), ("admit_ms", C.c_double),
+                ("device_ms", C.c_double), ("total_ms", C.c_double), ("batch_size", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("failed", C.c_int64), ("pixels", C.c_int64),
+                ("batches", C.c_int64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("max_ms", C.c_double), ("mpx_per_s", C.c_double),
+                ("peak_admitted_bytes", C.c_size_t)]
+
+
 class Job(C.Structure):
     _fields_ = [
         ("pixels", C.c_void_p),
@@ -106,6 +132,11 @@ SIGNATURES = {
     "rdb_context_destroy": (None, [C.c_void_p]),
     "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
     "rdb_context_last_passes": (C.c_int, [C.c_void_p]),
+    "rdb_server_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "rdb_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
+    "rdb_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p]),
+    "rdb_server_stats_get": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rdb_server_destroy": (None, [C.c_void_p]),
     "rdb_max_frames": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t]),
     "rdb_context_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "rdb_context_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -433,3 +464,63 @@ def inverse_filter(taps: int, diffusion: float = 1.0) -> np.ndarray:
 
 def block_gap(width: int, height: int) -> int:
     return int(load().rdb_block_gap(width, height))
+
+
+class Server:
+    """The request loop (rdb_server_*): submit host images with a colour count
+    and an engine from any thread; the server builds palettes on host
+    threads, admits by device memory and batches on its device workers."""
+
+    def __init__(self, device: int = 0, budget: int = 0, workers: int = 0, max_batch: int = 0,
+                 host_threads: int = 0):
+        o = ServerOptions(device, budget, workers, max_batch, host_threads)
+        self.handle = C.c_void_p()
+        _check(load().rdb_server_create(C.byref(o), C.byref(self.handle)))
+        self._live: dict[int, tuple] = {}
+
+    def submit(self, img: np.ndarray, colors: int, engine: str | int = "seq",
+               alpha: bool = False, rgba: bool = False, **opts) -> int:
+        img = np.ascontiguousarray(img)
+        h, w = img.shape[:2]
+        idx = np.zeros((h, w), np.uint8)
+        out = np.zeros((h, w, 4), np.float32) if rgba else None
+        r = Request()
+        r.pixels = _ptr(img)
+        r.row_stride = 0
+        r.width, r.height, r.layout = w, h, layout_of(img)
+        r.colors = colors
+        r.associate_alpha = int(alpha)
+        r.engine = ENGINES[engine] if isinstance(engine, str) else engine
+        r.options = options(**opts)
+        r.indices = _ptr(idx)
+        r.rgba_out = _ptr(out) if out is not None else None
+        t = C.c_uint64()
+        _check(load().rdb_server_submit(self.handle, C.byref(r), C.byref(t)))
+        self._live[t.value] = (img, idx, out, r)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(indices, rgba or None, timings dict) of one request."""
+        res = RequestResult()
+        rc = load().rdb_server_wait(self.handle, ticket, timeout_ms, C.byref(res))
+        if rc == 6:  # RDB_E_TIMEOUT: still running, buffers stay alive
+            raise TimeoutError(ticket)
+        _, idx, out, _ = self._live.pop(ticket)
+        _check(rc)
+        return idx, out, {f: getattr(res, f) for f, _ in RequestResult._fields_}
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(load().rdb_server_stats_get(self.handle, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            load().rdb_server_destroy(self.handle)
+            self.handle = None
+            self._live.clear()
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.rdb_server_destroy(self.handle)
+            self.handle = None

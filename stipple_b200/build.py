@@ -36,6 +36,7 @@ SOURCES = [
     "rdb_plan.cpp",
     "rdb_runtime.cpp",
     "rdb_capi.cpp",
+    "rdb_serve.cpp",
     "rdb_curve.cu",
     "rdb_walk_seq.cu",
     "rdb_walk_blocks.cu",

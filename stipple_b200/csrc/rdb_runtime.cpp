@@ -46,6 +46,7 @@ Context::~Context() {
     cudaFree(p.second.dev);
     cudaFree(p.second.uniform);
   }
+  for (auto& b : free_blocks_) cudaFree(b.second);
   for (auto& o : orders_) cudaFree(o.second);
   for (DevBuf* b : {&memo_, &memo_gen_, &seq_items_, &counter_, &status_, &curve_scratch_,
                     &block_images_, &block_offsets_, &block_cx_, &block_chosen_, &jac_cx_,
@@ -135,6 +136,33 @@ int Context::Reserve(DevBuf* b, std::size_t bytes, const char* what) {
   return RDB_OK;
 }
 
+void* Context::AllocBlock(std::size_t bytes, const char* what, int* rc) {
+  auto it = free_blocks_.find(bytes);
+  if (it != free_blocks_.end()) {
+    void* p = it->second;
+    free_blocks_.erase(it);
+    *rc = RDB_OK;
+    return p;
+  }
+  if (bytes_ + bytes > budget_) {
+    *rc = Fail(RDB_E_NOMEM, std::string(what) + ": budget exceeded");
+    return nullptr;
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    *rc = CudaFail(e, what);
+    return nullptr;
+  }
+  bytes_ += bytes;
+  *rc = RDB_OK;
+  return p;
+}
+
+void Context::FreeBlock(void* p, std::size_t bytes) {
+  if (p) free_blocks_.emplace(bytes, p);
+}
+
 int Context::CreatePalette(const PlanInput& in, int* id) {
   DevPlan p;
   const std::string err = BuildPlan(in, &p.host);
@@ -143,32 +171,33 @@ int Context::CreatePalette(const PlanInput& in, int* id) {
   p.smem = h->smem_bytes;
   p.count = h->count;
   p.assoc = h->assoc != 0;
-  if (bytes_ + p.host.size() > budget_) return Fail(RDB_E_NOMEM, "palette: budget exceeded");
-  cudaError_t e = cudaMalloc(&p.dev, p.host.size());
-  if (e != cudaSuccess) return CudaFail(e, "palette upload");
-  e = cudaMemcpy(p.dev, p.host.data(), p.host.size(), cudaMemcpyHostToDevice);
+  // Size classes of 16 KB keep recycled blocks interchangeable.
+  p.dev_bytes = (p.host.size() + 16383) & ~static_cast<std::size_t>(16383);
+  int rc = RDB_OK;
+  p.dev = static_cast<unsigned char*>(AllocBlock(p.dev_bytes, "palette", &rc));
+  if (!p.dev) return rc;
+  // Ordered on the context stream, complete before any other stream can use it.
+  cudaError_t e = cudaMemcpyAsync(p.dev, p.host.data(), p.host.size(), cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) {
-    cudaFree(p.dev);
+    FreeBlock(p.dev, p.dev_bytes);
     return CudaFail(e, "palette upload");
   }
-  bytes_ += p.host.size();
   const int pid = next_palette_++;
   plans_[pid] = std::move(p);
   *id = pid;
   return RDB_OK;
 }
 
+// The caller has finished (synchronised) every stream other than the
+// context's own on which it used the palette; the context's own stream is
+// drained here.  Its blocks go back to the context's pool.
 int Context::DestroyPalette(int id) {
   auto it = plans_.find(id);
   if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
   cudaStreamSynchronize(stream_);
-  cudaFree(it->second.dev);
-  bytes_ -= it->second.host.size();
-  if (it->second.uniform) {
-    cudaDeviceSynchronize();  // any stream may still read it
-    cudaFree(it->second.uniform);
-    bytes_ -= kUniformKeys;
-  }
+  FreeBlock(it->second.dev, it->second.dev_bytes);
+  FreeBlock(it->second.uniform, kUniformKeys);
   plans_.erase(it);
   return RDB_OK;
 }
@@ -179,14 +208,11 @@ int Context::Uniform(int id, cudaStream_t s, const uint8_t** out) {
   DevPlan& p = it->second;
   if (p.assoc) return Fail(RDB_E_UNSUPPORTED, "uniform-key table: alpha-associated palette");
   if (!p.uniform) {
-    if (bytes_ + kUniformKeys > budget_) return Fail(RDB_E_NOMEM, "uniform-key table: budget exceeded");
-    cudaError_t e = cudaMalloc(&p.uniform, kUniformKeys);
-    if (e != cudaSuccess) {
-      p.uniform = nullptr;
-      return CudaFail(e, "uniform-key table");
-    }
-    bytes_ += kUniformKeys;
+    int rc = RDB_OK;
+    p.uniform = static_cast<uint8_t*>(AllocBlock(kUniformKeys, "uniform-key table", &rc));
+    if (!p.uniform) return rc;
     // Built once; other streams may read it later, so it is complete on return.
+    cudaError_t e;
     if ((e = LaunchUniformTable(p.dev, p.uniform, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess) {
       return CudaFail(e, "uniform-key table");

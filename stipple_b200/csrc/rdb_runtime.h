@@ -32,6 +32,7 @@ struct DevBuf {
 
 struct DevPlan {
   unsigned char* dev = nullptr;
+  std::size_t dev_bytes = 0;
   std::vector<uint8_t> host;
   int smem = 0;
   int count = 0;
@@ -74,6 +75,12 @@ class Context {
   int Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int CheckJob(const rdb_job& j) const;
   void Release(DevBuf* b);
+  // Small per-palette device blocks are recycled instead of freed: cudaFree
+  // waits for the whole device, which would stall every other stream's work
+  // each time a request's palette is dropped.
+  void* AllocBlock(std::size_t bytes, const char* what, int* rc);
+  void FreeBlock(void* p, std::size_t bytes);
+  std::multimap<std::size_t, void*> free_blocks_;
 
   int device_ = 0;
   int sm_count_ = 148;

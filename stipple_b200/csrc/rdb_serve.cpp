@@ -1,0 +1,356 @@
+// rdb_serve.cpp -- the request loop declared in include/rdb.h (rdb_server_*).
+//
+// Three stages, each its own threads, joined by queues under one mutex:
+//   build    host threads turn a request into a colour tree (rdb_octree_build,
+//            the reference's ColorTree::Build semantics, greyscale rule of
+//            src/rd_cli.cpp:2452-2456) -- the CPU-heavy part, parallel by
+//            request;
+//   admit    a built request waits until the device-memory estimate of all
+//            admitted requests plus its own fits the budget (first fit in
+//            arrival order, so one large request does not block small ones
+//            behind it forever: it is taken as soon as it fits);
+//   device   each worker owns a context and its stream; when idle it takes
+//            every admitted request that shares the oldest one's engine and
+//            options (and, for the block engine, its palette tree) as one
+//            batched call, so arrivals during a batch form the next batch on
+//            whichever worker frees first.
+// A request's result does not depend on its batch: every engine treats the
+// jobs of a call independently.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/rdb.h"
+#include "rdb_runtime.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double Ms(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Req {
+  rdb_request r{};
+  uint64_t ticket = 0;
+  Clock::time_point t_submit, t_built, t_start, t_done;
+  rdb_octree* tree = nullptr;
+  std::size_t bytes = 0;
+  int status = RDB_OK;
+  bool done = false;
+  int batch = 0;
+  double device_ms = 0.0;
+};
+
+// Device bytes one request needs while admitted: staging of input, indices and
+// RgbaF output, plus its engine's scratch (the segmented walk's samples,
+// memo tables, queues and key maps; the block and Jacobi copies).
+std::size_t EstimateBytes(const rdb_request& r) {
+  const std::size_t px = static_cast<std::size_t>(r.width) * r.height;
+  std::size_t b = px * (rdb::BytesPerPixel(r.layout) + 1 + (r.rgba_out ? 16 : 0)) + 4 * px;
+  if (r.engine == RDB_ENGINE_SEQ) {
+    b += px * 64 + (std::size_t{3} << 20) + (r.associate_alpha ? px * 16 : 0);
+  } else {
+    b += px * 24;
+  }
+  return b + (std::size_t{1} << 20);
+}
+
+bool SameOptions(const rdb_options& a, const rdb_options& b) {
+  return std::memcmp(&a, &b, sizeof(rdb_options)) == 0;
+}
+
+}  // namespace
+
+struct rdb_server {
+  rdb_server_options o{};
+  std::size_t budget = 0;
+  std::mutex mu;
+  std::condition_variable cv_build, cv_ready, cv_done;
+  std::deque<Req*> incoming;
+  std::deque<Req*> ready;
+  std::unordered_map<uint64_t, Req*> all;
+  uint64_t next_ticket = 1;
+  std::size_t admitted = 0;
+  bool stop = false;
+  int pending = 0;  // submitted, not yet completed
+  std::vector<std::thread> builders, workers;
+  // statistics
+  std::vector<double> latencies;
+  int64_t failed = 0, pixels = 0, batches = 0;
+  bool any = false;
+  Clock::time_point first_submit, last_done;
+  std::size_t peak = 0;
+
+  void Build();
+  void Work(int index);
+  std::vector<Req*> TakeBatch();
+};
+
+void rdb_server::Build() {
+  for (;;) {
+    Req* q = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_build.wait(lk, [&] { return stop || !incoming.empty(); });
+      if (incoming.empty()) return;
+      q = incoming.front();
+      incoming.pop_front();
+    }
+    const rdb_request& r = q->r;
+    const int gray = rdb_is_grayscale(r.pixels, r.layout, r.width, r.height, r.row_stride);
+    const int rc = rdb_octree_build(r.pixels, r.layout, r.width, r.height, r.row_stride, r.colors,
+                                    r.associate_alpha, gray, &q->tree);
+    std::lock_guard<std::mutex> lk(mu);
+    q->t_built = Clock::now();
+    if (rc != RDB_OK) {
+      q->status = rc;
+      q->done = true;
+      q->t_done = q->t_built;
+      ++failed;
+      --pending;
+      cv_done.notify_all();
+      continue;
+    }
+    ready.push_back(q);
+    cv_ready.notify_all();
+  }
+}
+
+// Under the lock: the oldest admissible request and every other admissible
+// request compatible with it, admitted now.
+std::vector<Req*> rdb_server::TakeBatch() {
+  std::vector<Req*> batch;
+  Req* head = nullptr;
+  for (Req* q : ready) {
+    if (admitted + q->bytes <= budget || admitted == 0) {
+      head = q;
+      break;
+    }
+  }
+  if (!head) return batch;
+  const int max_batch = o.max_batch > 0 ? o.max_batch : 512;
+  for (auto it = ready.begin(); it != ready.end() && static_cast<int>(batch.size()) < max_batch;) {
+    Req* q = *it;
+    const bool compatible = q == head ||
+                            (q->r.engine == head->r.engine && SameOptions(q->r.options, head->r.options) &&
+                             q->r.engine != RDB_ENGINE_BLOCKS);
+    if (compatible && (admitted + q->bytes <= budget || (admitted == 0 && q == head))) {
+      admitted += q->bytes;
+      batch.push_back(q);
+      it = ready.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  peak = std::max(peak, admitted);
+  return batch;
+}
+
+void rdb_server::Work(int index) {
+  rdb_context* ctx = nullptr;
+  const std::size_t share = budget / static_cast<std::size_t>(std::max(1, o.workers));
+  cudaSetDevice(o.device);
+  const int crc = rdb_context_create(o.device, share, &ctx);
+  (void)index;
+  for (;;) {
+    std::vector<Req*> batch;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_ready.wait(lk, [&] {
+        if (stop && ready.empty() && incoming.empty() && pending == 0) return true;
+        if (ready.empty()) return false;
+        batch = TakeBatch();
+        return !batch.empty();
+      });
+      if (batch.empty()) break;
+    }
+    const Clock::time_point t0 = Clock::now();
+    std::vector<int> pids(batch.size(), 0);
+    std::vector<rdb_host_job> jobs(batch.size());
+    int rc = crc;
+    for (std::size_t i = 0; i < batch.size() && rc == RDB_OK; ++i) {
+      rc = rdb_palette_from_octree(ctx, batch[i]->tree, &pids[i]);
+      const rdb_request& r = batch[i]->r;
+      rdb_host_job& j = jobs[i];
+      j.pixels = r.pixels;
+      j.row_stride = r.row_stride;
+      j.width = r.width;
+      j.height = r.height;
+      j.layout = r.layout;
+      j.palette_id = pids[i];
+      j.indices = r.indices;
+      j.rgba_out = r.rgba_out;
+    }
+    if (rc == RDB_OK) {
+      rc = rdb_dither_host(ctx, batch[0]->r.engine, jobs.data(), static_cast<int>(jobs.size()),
+                           &batch[0]->r.options);
+    }
+    for (int pid : pids) {
+      if (pid) rdb_palette_destroy(ctx, pid);
+    }
+    const Clock::time_point t1 = Clock::now();
+    std::lock_guard<std::mutex> lk(mu);
+    ++batches;
+    for (Req* q : batch) {
+      rdb_octree_free(q->tree);
+      q->tree = nullptr;
+      q->status = rc;
+      q->t_start = t0;
+      q->t_done = t1;
+      q->device_ms = Ms(t0, t1);
+      q->batch = static_cast<int>(batch.size());
+      q->done = true;
+      admitted -= q->bytes;
+      --pending;
+      if (rc == RDB_OK) {
+        latencies.push_back(Ms(q->t_submit, t1));
+        pixels += static_cast<int64_t>(q->r.width) * q->r.height;
+        last_done = t1;
+      } else {
+        ++failed;
+      }
+    }
+    cv_done.notify_all();
+    cv_ready.notify_all();  // memory freed: other workers may admit now
+  }
+  if (ctx) rdb_context_destroy(ctx);
+}
+
+extern "C" {
+
+int rdb_server_create(const rdb_server_options* opts, rdb_server** out) {
+  if (!out) return rdb::Fail(RDB_E_INVALID, "rdb_server_create: null output");
+  rdb_server* s = new rdb_server();
+  if (opts) s->o = *opts;
+  if (s->o.workers <= 0) s->o.workers = 4;
+  if (s->o.host_threads <= 0) s->o.host_threads = std::max(1u, std::thread::hardware_concurrency());
+  if (cudaSetDevice(s->o.device) != cudaSuccess) {
+    delete s;
+    return rdb::Fail(RDB_E_CUDA, "rdb_server_create: no such device");
+  }
+  std::size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    delete s;
+    return rdb::Fail(RDB_E_CUDA, "rdb_server_create: cudaMemGetInfo failed");
+  }
+  s->budget = s->o.memory_budget ? std::min(s->o.memory_budget, (free_b / 10) * 9) : (free_b / 10) * 9;
+  for (int i = 0; i < s->o.host_threads; ++i) s->builders.emplace_back([s] { s->Build(); });
+  for (int i = 0; i < s->o.workers; ++i) s->workers.emplace_back([s, i] { s->Work(i); });
+  *out = s;
+  return RDB_OK;
+}
+
+int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
+  if (!s || !req || !ticket) return rdb::Fail(RDB_E_INVALID, "rdb_server_submit: null argument");
+  if (!req->pixels || !req->indices || req->width < 1 || req->height < 1) {
+    return rdb::Fail(RDB_E_INVALID, "rdb_server_submit: bad request");
+  }
+  if (req->engine < RDB_ENGINE_SEQ || req->engine > RDB_ENGINE_JACOBI) {
+    return rdb::Fail(RDB_E_INVALID, "rdb_server_submit: unknown engine");
+  }
+  Req* q = new Req();
+  q->r = *req;
+  q->bytes = EstimateBytes(*req);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) {
+    delete q;
+    return rdb::Fail(RDB_E_INVALID, "rdb_server_submit: server is stopping");
+  }
+  if (q->bytes > s->budget) {
+    delete q;
+    return rdb::Fail(RDB_E_NOMEM, "rdb_server_submit: request larger than the admission budget");
+  }
+  q->ticket = s->next_ticket++;
+  q->t_submit = Clock::now();
+  if (!s->any) {
+    s->any = true;
+    s->first_submit = q->t_submit;
+  }
+  s->all[q->ticket] = q;
+  s->incoming.push_back(q);
+  ++s->pending;
+  *ticket = q->ticket;
+  s->cv_build.notify_one();
+  return RDB_OK;
+}
+
+int rdb_server_wait(rdb_server* s, uint64_t ticket, int timeout_ms, rdb_request_result* out) {
+  if (!s) return rdb::Fail(RDB_E_INVALID, "rdb_server_wait: null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return rdb::Fail(RDB_E_INVALID, "rdb_server_wait: unknown ticket");
+  Req* q = it->second;
+  const auto done = [&] { return q->done; };
+  if (timeout_ms < 0) {
+    s->cv_done.wait(lk, done);
+  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), done)) {
+    return rdb::Fail(RDB_E_TIMEOUT, "rdb_server_wait: not done yet");
+  }
+  if (out) {
+    out->status = q->status;
+    out->queue_ms = Ms(q->t_submit, q->t_built);
+    out->admit_ms = q->t_start > q->t_built ? Ms(q->t_built, q->t_start) : 0.0;
+    out->device_ms = q->device_ms;
+    out->total_ms = Ms(q->t_submit, q->t_done);
+    out->batch_size = q->batch;
+  }
+  s->all.erase(it);
+  const int st = q->status;
+  delete q;
+  if (st != RDB_OK) return rdb::Fail(st, "rdb_server_wait: the request failed");
+  return RDB_OK;
+}
+
+int rdb_server_stats_get(rdb_server* s, rdb_server_stats* out) {
+  if (!s || !out) return rdb::Fail(RDB_E_INVALID, "rdb_server_stats_get: null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(out, 0, sizeof(*out));
+  out->completed = static_cast<int64_t>(s->latencies.size());
+  out->failed = s->failed;
+  out->pixels = s->pixels;
+  out->batches = s->batches;
+  out->peak_admitted_bytes = s->peak;
+  if (!s->latencies.empty()) {
+    std::vector<double> v = s->latencies;
+    std::sort(v.begin(), v.end());
+    const auto pct = [&](double p) {
+      const std::size_t k = static_cast<std::size_t>(p * static_cast<double>(v.size() - 1) + 0.5);
+      return v[std::min(k, v.size() - 1)];
+    };
+    out->p50_ms = pct(0.50);
+    out->p99_ms = pct(0.99);
+    out->max_ms = v.back();
+    const double span = Ms(s->first_submit, s->last_done);
+    out->mpx_per_s = span > 0 ? static_cast<double>(s->pixels) / (span * 1e3) : 0.0;
+  }
+  return RDB_OK;
+}
+
+void rdb_server_destroy(rdb_server* s) {
+  if (!s) return;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait(lk, [&] { return s->pending == 0; });
+    s->stop = true;
+  }
+  s->cv_build.notify_all();
+  s->cv_ready.notify_all();
+  for (std::thread& t : s->builders) t.join();
+  for (std::thread& t : s->workers) t.join();
+  for (auto& kv : s->all) {
+    rdb_octree_free(kv.second->tree);
+    delete kv.second;
+  }
+  delete s;
+}
+
+}  // extern "C"

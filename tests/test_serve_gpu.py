@@ -1,0 +1,89 @@
+"""The request loop (rdb_server_*): a mixed stream of sizes, palettes, layouts
+and engines submitted concurrently gives every request the same bytes as the
+same request alone; admission keeps within a tight budget; requests larger
+than the budget are refused at submission."""
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+import stipple_b200 as sb
+from stipple_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix(n, seed):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n):
+        w = int(np.exp(rng.uniform(np.log(8), np.log(700))))
+        h = int(np.exp(rng.uniform(np.log(8), np.log(500))))
+        alpha = bool(rng.random() < 0.4)
+        img = synth.gradient_rgba8(w, h, 500 + k) if alpha else synth.gradient_rgb8(w, h, 500 + k)
+        colors = int(rng.choice([2, 4, 8, 16, 64, 256]))
+        engine = str(rng.choice(["seq", "seq", "seq", "blocks", "blocks", "jacobi"]))
+        reqs.append((img, colors, engine, alpha))
+    return reqs
+
+
+def _alone(ctx, img, colors, engine, alpha):
+    t = sb.Octree(img, colors, alpha)
+    pid = ctx.palette_from_octree(t)
+    try:
+        return ctx.dither_host(engine, img, pid, rgba=True)
+    finally:
+        ctx.release_palette(pid)
+
+
+def test_mixed_stream_equals_each_request_alone(ctx):
+    reqs = _mix(48, 3)
+    srv = sb.Server(workers=3, max_batch=16)
+    try:
+        tickets = [None] * len(reqs)
+
+        def submit(lo, hi):
+            for k in range(lo, hi):
+                img, colors, engine, alpha = reqs[k]
+                tickets[k] = srv.submit(img, colors, engine, alpha=alpha, rgba=True)
+
+        th = [threading.Thread(target=submit, args=(i * 16, (i + 1) * 16)) for i in range(3)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        results = [srv.wait(t) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+    assert st["batches"] < len(reqs)  # something was batched
+    for k, (img, colors, engine, alpha) in enumerate(reqs):
+        idx, rgba, info = results[k]
+        want_idx, want_rgba = _alone(ctx, img, colors, engine, alpha)
+        assert np.array_equal(idx, want_idx), (k, engine, img.shape)
+        assert np.array_equal(rgba.view(np.uint32), want_rgba.view(np.uint32)), (k, engine)
+        assert info["status"] == 0 and info["total_ms"] >= info["device_ms"]
+
+
+def test_admission_budget(ctx):
+    reqs = _mix(12, 7)
+    # Room for roughly one mid-size request at a time: everything still
+    # completes, never more than the budget admitted at once.
+    budget = 96 << 20
+    srv = sb.Server(workers=2, budget=budget)
+    try:
+        tickets = [srv.submit(img, c, e, alpha=a) for img, c, e, a in reqs]
+        outs = [srv.wait(t)[0] for t in tickets]
+        st = srv.stats()
+        assert st["peak_admitted_bytes"] <= budget
+        big = synth.gradient_rgb8(4096, 4096, 1)
+        with pytest.raises(sb.RdbError):
+            srv.submit(big, 16, "seq")
+    finally:
+        srv.close()
+    for (img, c, e, a), idx in zip(reqs, outs):
+        assert np.array_equal(idx, _alone(ctx, img, c, e, a)[0])
