@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--block-frames", type=int, default=16)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--skip-extra", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=160,
+                    help="requests in the served-stream sample (the full stream is 10,000)")
+    ap.add_argument("--serve-rates", default="20,60",
+                    help="Poisson arrival rates (requests/s) of the served-stream sample")
     ap.add_argument("--profile-case", default="none", choices=["none", "seq", "blocks"],
                     help="run only that workload's device steps (for ncu captures) and print "
                          "its timing; no JSON contract line")
@@ -267,6 +271,7 @@ def run_ours(a, rank: int, world: int):
     if rank == 0 and not a.skip_extra:
         out["blocks"] = bench_blocks(ctx, s, a, tree, pid, hbm)
         out["batched"] = bench_batched(ctx, s, a)
+        out["serve"] = bench_serve(ctx, a)
     if rank == 0:
         cpu, _ = reference_cpu(img, C, budget_s=12.0)
         out["cpu_baseline"] = cpu
@@ -341,6 +346,75 @@ def bench_batched(ctx, s, a):
             "batched_ms": ms_b, "batched_mpx_s": total / ms_b / 1e3,
             "plain_ms": ms_p, "plain_mpx_s": total / ms_p / 1e3,
             "speedup": ms_p / ms_b, "amdahl_cap": total / biggest}
+
+
+def bench_serve(ctx, a):
+    """Served mixed stream (a sample of the 10,000-request stream): Poisson
+    arrivals at each rate, W and H log-uniform in 64..4096, RGB8 or RGBA8 (half
+    each, alpha-associated palettes for RGBA), colours from {2, 4, ..., 256},
+    engines 60 % sequential / 30 % block / 10 % Jacobi, admission capped at
+    120 GB.  Latency = submission to result in host memory (palette build,
+    admission wait, upload, dither, download).  Beside it, the plain form: the
+    same requests one at a time, one call each, on one context."""
+    import stipple_b200 as sb
+    from stipple_b200 import synth
+    rng = np.random.default_rng(77)
+    n = a.serve_requests
+    sizes = synth.log_uniform_sizes(n, seed=78, lo=64, hi=4096)
+    # Requests are crops of two seeded 4096x4096 frames at random offsets (the
+    # generator costs ~0.2 us per pixel; cropping keeps the sample cheap).
+    base = {False: synth.gradient_rgb8(4096, 4096, 3000), True: synth.gradient_rgba8(4096, 4096, 3001)}
+    reqs = []
+    for k, (w, h) in enumerate(sizes):
+        alpha = bool(rng.random() < 0.5)
+        y0 = int(rng.integers(0, 4096 - h + 1))
+        x0 = int(rng.integers(0, 4096 - w + 1))
+        img = np.ascontiguousarray(base[alpha][y0:y0 + h, x0:x0 + w])
+        colors = int(rng.choice([2, 4, 8, 16, 32, 64, 128, 256]))
+        u = rng.random()
+        engine = "seq" if u < 0.6 else ("blocks" if u < 0.9 else "jacobi")
+        reqs.append((img, colors, engine, alpha))
+    total_px = sum(w * h for w, h in sizes)
+    out = {"requests": n, "total_px": total_px,
+           "workload": "served mixed stream sample: sizes log-uniform 64..4096, RGB/RGBA8, "
+                       "2..256 colours, 60/30/10 seq/block/Jacobi, 120 GB admission"}
+    rates = [float(r) for r in a.serve_rates.split(",") if r]
+    for rate in rates:
+        srv = sb.Server(budget=120 << 30, workers=4)
+        gaps = rng.exponential(1.0 / rate, size=n)
+        t0 = time.perf_counter()
+        due = t0
+        tickets = []
+        for (img, colors, engine, alpha), g in zip(reqs, gaps):
+            due += g
+            now = time.perf_counter()
+            if due > now:
+                time.sleep(due - now)
+            tickets.append(srv.submit(img, colors, engine, alpha=alpha))
+        for t in tickets:
+            srv.wait(t)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        out[f"rate_{rate:g}"] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                                 "max_ms": st["max_ms"], "mpx_s": st["mpx_per_s"],
+                                 "batches": st["batches"], "wall_s": wall,
+                                 "peak_admitted_gb": st["peak_admitted_bytes"] / 2**30}
+    # Plain per-request form on the same requests.
+    lat = []
+    t0 = time.perf_counter()
+    for img, colors, engine, alpha in reqs:
+        t1 = time.perf_counter()
+        tr = sb.Octree(img, colors, alpha)
+        pid = ctx.palette_from_octree(tr)
+        ctx.dither_host(engine, img, pid)
+        ctx.release_palette(pid)
+        lat.append((time.perf_counter() - t1) * 1e3)
+    plain_s = time.perf_counter() - t0
+    out["plain"] = {"mpx_s": total_px / plain_s / 1e6, "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99)), "wall_s": plain_s,
+                    "note": "service time per request, no queueing"}
+    return out
 
 
 # ---------------------------------------------------------------- reference arm

@@ -4,12 +4,31 @@
 // in source order, as in the reference CPU walk (src/rd_riemersma_cpu.cpp).
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "rdb_numeric.h"
 #include "rdb_plan.h"
 
 namespace rdb {
+
+// Raises a kernel's dynamic shared-memory cap to all the device allows.  The
+// cap is process-wide per kernel: setting it to one launch's own size would
+// race with another host thread launching the same kernel with a larger size
+// in between (that launch then fails with an invalid argument).  The maximum
+// is the same value for every caller.
+template <typename Kernel>
+inline cudaError_t AllowMaxSmem(Kernel kernel) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - static_cast<int>(fa.sharedSizeBytes));
+}
 
 // Error codes a kernel can leave in its status word.
 enum DeviceStatus : int {

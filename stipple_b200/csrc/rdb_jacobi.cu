@@ -181,15 +181,13 @@ template <typename T>
 cudaError_t Run(const JacobiLaunch& L, cudaStream_t stream) {
   const unsigned g = static_cast<unsigned>((L.n + 255) / 256);
   JacobiGather<T><<<g, 256, 0, stream>>>(L);
-  cudaError_t e = cudaFuncSetAttribute(JacobiInit<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       L.plan_smem);
+  cudaError_t e = AllowMaxSmem(JacobiInit<T>);
   if (e != cudaSuccess) return e;
   JacobiInit<T><<<g, 256, L.plan_smem, stream>>>(L);
   const std::size_t smem = static_cast<std::size_t>(L.plan_smem) +
                            sizeof(T) * 4 * static_cast<std::size_t>(kTile + L.taps) +
                            sizeof(T) * static_cast<std::size_t>(L.taps + 1);
-  e = cudaFuncSetAttribute(JacobiSweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
+  e = AllowMaxSmem(JacobiSweep<T>);
   if (e != cudaSuccess) return e;
   const unsigned tiles = static_cast<unsigned>((L.n + kTile - 1) / kTile);
   uint8_t* a = L.q0;

@@ -48,6 +48,7 @@ struct Req {
   bool done = false;
   int batch = 0;
   double device_ms = 0.0;
+  std::string err;
 };
 
 // Device bytes one request needs while admitted: staging of input, indices and
@@ -113,6 +114,7 @@ void rdb_server::Build() {
     q->t_built = Clock::now();
     if (rc != RDB_OK) {
       q->status = rc;
+      q->err = std::string("palette build: ") + rdb_last_error();
       q->done = true;
       q->t_done = q->t_built;
       ++failed;
@@ -194,6 +196,7 @@ void rdb_server::Work(int index) {
       rc = rdb_dither_host(ctx, batch[0]->r.engine, jobs.data(), static_cast<int>(jobs.size()),
                            &batch[0]->r.options);
     }
+    const std::string err = rc == RDB_OK ? std::string() : std::string(rdb_last_error());
     for (int pid : pids) {
       if (pid) rdb_palette_destroy(ctx, pid);
     }
@@ -208,6 +211,7 @@ void rdb_server::Work(int index) {
       q->t_done = t1;
       q->device_ms = Ms(t0, t1);
       q->batch = static_cast<int>(batch.size());
+      q->err = err;
       q->done = true;
       admitted -= q->bytes;
       --pending;
@@ -305,8 +309,9 @@ int rdb_server_wait(rdb_server* s, uint64_t ticket, int timeout_ms, rdb_request_
   }
   s->all.erase(it);
   const int st = q->status;
+  const std::string err = q->err;
   delete q;
-  if (st != RDB_OK) return rdb::Fail(st, "rdb_server_wait: the request failed");
+  if (st != RDB_OK) return rdb::Fail(st, "rdb_server_wait: the request failed: " + err);
   return RDB_OK;
 }
 

@@ -475,8 +475,7 @@ std::size_t SswSmemBytes(int plan_smem_max, int cache_bits) {
 
 cudaError_t LaunchSswWalk(const SswLaunch& L, int grid, cudaStream_t s) {
   const std::size_t smem = SswSmemBytes(L.plan_smem_max, L.cache_bits);
-  cudaError_t e = cudaFuncSetAttribute(SswWalkKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = AllowMaxSmem(SswWalkKernel);
   if (e != cudaSuccess) return e;
   SswWalkKernel<<<grid, 32, smem, s>>>(L);
   return cudaGetLastError();

@@ -426,8 +426,7 @@ std::size_t TswSmemBytes(int plan_smem_max) {
 
 int TswResidentThreads(int plan_smem_max, int sm_count) {
   const int smem = static_cast<int>(TswSmemBytes(plan_smem_max));
-  if (cudaFuncSetAttribute(TswWalkKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-      cudaSuccess) {
+  if (AllowMaxSmem(TswWalkKernel<false>) != cudaSuccess) {
     return 0;
   }
   int blocks = 0;
@@ -455,11 +454,11 @@ cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s) {
   const int smem = static_cast<int>(TswSmemBytes(L.plan_smem_max));
   cudaError_t e;
   if (L.is_float) {
-    e = cudaFuncSetAttribute(TswWalkKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = AllowMaxSmem(TswWalkKernel<true>);
     if (e != cudaSuccess) return e;
     TswWalkKernel<true><<<L.n_chunks, L.chunk_threads, smem, s>>>(L);
   } else {
-    e = cudaFuncSetAttribute(TswWalkKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = AllowMaxSmem(TswWalkKernel<false>);
     if (e != cudaSuccess) return e;
     TswWalkKernel<false><<<L.n_chunks, L.chunk_threads, smem, s>>>(L);
   }

@@ -231,8 +231,7 @@ __global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaun
 
 template <bool kAssoc, bool kFloat>
 cudaError_t LaunchWalk(const BlockLaunch& L, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(BlockWalkKernel<kAssoc, kFloat>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L.plan_smem);
+  cudaError_t e = AllowMaxSmem(BlockWalkKernel<kAssoc, kFloat>);
   if (e != cudaSuccess) return e;
   const unsigned g2 = static_cast<unsigned>((L.total_blocks + 127) / 128);
   BlockWalkKernel<kAssoc, kFloat><<<g2, 128, L.plan_smem, stream>>>(L);

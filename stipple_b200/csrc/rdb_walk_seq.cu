@@ -297,8 +297,7 @@ std::size_t SeqSmemBytes(int plan_smem_max, int cache_bits, bool use_cache) {
 
 cudaError_t LaunchSeqWalk(const SeqLaunch& L, int grid, cudaStream_t stream) {
   const std::size_t smem = SeqSmemBytes(L.plan_smem_max, L.cache_bits, L.use_cache != 0);
-  cudaError_t e = cudaFuncSetAttribute(SeqWalkKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = AllowMaxSmem(SeqWalkKernel);
   if (e != cudaSuccess) return e;
   SeqWalkKernel<<<grid, 32, smem, stream>>>(L);
   return cudaGetLastError();
