@@ -34,6 +34,10 @@ int Fail(int code, const std::string& msg) {
   return code;
 }
 
+std::string CudaErr(cudaError_t e, const char* what) {
+  return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
 int CudaFail(cudaError_t e, const char* what) {
   return Fail(e == cudaErrorMemoryAllocation ? RDB_E_NOMEM : RDB_E_CUDA,
               std::string(what) + ": " + cudaGetErrorString(e));
@@ -59,7 +63,46 @@ Context::~Context() {
   for (cudaEvent_t& ev : ev_) {
     if (ev) cudaEventDestroy(ev);
   }
+  for (cudaEvent_t ev : pass_ev_) cudaEventDestroy(ev);
+  if (scratch_ev_) cudaEventDestroy(scratch_ev_);
+  for (cudaEvent_t ev : walk_ev_) cudaEventDestroy(ev);
+  if (ring_h_) cudaFreeHost(ring_h_);
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Context::PinnedRing(std::size_t ints) {
+  if (ring_cap_ >= ints) return RDB_OK;
+  if (ring_h_) {
+    cudaStreamSynchronize(stream_);
+    cudaFreeHost(ring_h_);
+    ring_h_ = nullptr;
+    ring_cap_ = 0;
+  }
+  const std::size_t want = std::max<std::size_t>(ints, 1024);
+  const cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&ring_h_), want * sizeof(int),
+                                      cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    ring_h_ = nullptr;
+    return CudaFail(e, "pinned pass results");
+  }
+  ring_cap_ = want;
+  return RDB_OK;
+}
+
+int Context::PassEvents(int depth) {
+  while (static_cast<int>(pass_ev_.size()) < depth) {
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return CudaFail(e, "pass events");
+    pass_ev_.push_back(ev);
+  }
+  while (static_cast<int>(walk_ev_.size()) < 2 * depth) {
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) return CudaFail(e, "walk events");
+    walk_ev_.push_back(ev);
+  }
+  return RDB_OK;
 }
 
 int Context::Profile(bool on) {
@@ -311,18 +354,36 @@ int Context::Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o
   }
   if (!s) s = stream_;
   cudaSetDevice(device_);
-  switch (engine) {
-    case RDB_ENGINE_SEQ: {
-      if (o.seq_mode == 1) return Seq(jobs, n, o, s);
-      if (o.seq_mode == 2) return SeqSegmented(jobs, n, o, s);
-      if (o.seq_mode == 3) return SeqThreadSegmented(jobs, n, o, s);
-      if (o.seq_mode != 0) return Fail(RDB_E_INVALID, "seq_mode must be 0..3");
-      return SeqAuto(jobs, n, o, s);
-    }
-    case RDB_ENGINE_BLOCKS: return Blocks(jobs, n, o, s);
-    case RDB_ENGINE_JACOBI: return Jacobi(jobs, n, o, s);
-    default: return Fail(RDB_E_INVALID, "unknown engine");
+  // The context's scratch buffers are shared by every call: a call on a new
+  // stream waits (on the device) for the work the previous call enqueued.
+  if (!scratch_ev_) {
+    const cudaError_t e = cudaEventCreateWithFlags(&scratch_ev_, cudaEventDisableTiming);
+    if (e != cudaSuccess) return CudaFail(e, "scratch event");
+  } else if (scratch_stream_ != s) {
+    cudaStreamWaitEvent(s, scratch_ev_, 0);
   }
+  int rc;
+  switch (engine) {
+    case RDB_ENGINE_SEQ:
+      if (o.seq_mode == 1) {
+        rc = Seq(jobs, n, o, s);
+      } else if (o.seq_mode == 2) {
+        rc = SeqSegmented(jobs, n, o, s);
+      } else if (o.seq_mode == 3) {
+        rc = SeqThreadSegmented(jobs, n, o, s);
+      } else if (o.seq_mode != 0) {
+        rc = Fail(RDB_E_INVALID, "seq_mode must be 0..3");
+      } else {
+        rc = SeqAuto(jobs, n, o, s);
+      }
+      break;
+    case RDB_ENGINE_BLOCKS: rc = Blocks(jobs, n, o, s); break;
+    case RDB_ENGINE_JACOBI: rc = Jacobi(jobs, n, o, s); break;
+    default: rc = Fail(RDB_E_INVALID, "unknown engine");
+  }
+  cudaEventRecord(scratch_ev_, s);
+  scratch_stream_ = s;
+  return rc;
 }
 
 int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
@@ -1001,49 +1062,68 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   }
   if ((e = LaunchTswGather(L, positions, s)) != cudaSuccess) return CudaFail(e, "sample gather");
 
-  std::vector<int> bad_h(static_cast<std::size_t>(n));
+  // Passes are enqueued up to kDepth ahead of the one the host is checking:
+  // every kernel takes its verified prefix from the device's own result of
+  // the previous pass, so the host only has to learn when to stop.  Each pass
+  // copies its per-image first failure and the status word into a pinned
+  // ring slot and records an event; passes enqueued past convergence find
+  // every segment verified and walk nothing.
+  constexpr int kDepth = 4;
+  const std::size_t slot_ints = static_cast<std::size_t>(n) + 1;
+  if (int rc = PinnedRing(kDepth * slot_ints)) return rc;
+  if (int rc = PassEvents(kDepth)) return rc;
   std::vector<int> front(static_cast<std::size_t>(n), -1);
   const int max_passes = o.max_passes > 0 ? o.max_passes : 1 << 30;
-  int pass = 0;
-  for (;; ++pass) {
-    if (pass >= max_passes) {
-      return Fail(RDB_E_DEVICE, "segmented walk did not converge within the pass limit");
+  const auto drain = [&](int code, const std::string& msg) {
+    cudaStreamSynchronize(s);
+    cudaMemset(status_.ptr, 0, sizeof(int));
+    return Fail(code, msg);
+  };
+  int issued = 0, checked = 0;
+  bool done = false;
+  while (!done) {
+    while (issued < checked + kDepth && issued < max_passes) {
+      const int k = issued % kDepth;
+      L.pass = issued;
+      L.tag = static_cast<uint32_t>(issued + 1);
+      int* cur = L.bad[issued & 1];
+      cudaMemsetAsync(cur, 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
+      if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "first-touch map"));
+      if (profiling_) cudaEventRecord(walk_ev_[2 * k], s);
+      if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "segmented walk"));
+      if (profiling_) cudaEventRecord(walk_ev_[2 * k + 1], s);
+      if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "verification"));
+      int* slot = ring_h_ + static_cast<std::size_t>(k) * slot_ints;
+      if ((e = cudaMemcpyAsync(slot, cur, static_cast<std::size_t>(n) * sizeof(int),
+                               cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(slot + n, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+          (e = cudaEventRecord(pass_ev_[k], s)) != cudaSuccess) {
+        return drain(RDB_E_CUDA, CudaErr(e, "verification readback"));
+      }
+      if (profiling_) stats_.launches += 1 + 1 + (use_cache ? 2 : 0);  // walk, checks, [prepare, keys]
+      ++issued;
     }
-    L.pass = pass;
-    L.tag = static_cast<uint32_t>(pass + 1);
-    int* cur = L.bad[pass & 1];
-    cudaMemsetAsync(cur, 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
-    if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
-    if (profiling_) cudaEventRecord(ev_[0], s);
-    if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
-    if (profiling_) cudaEventRecord(ev_[1], s);
-    if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
-    if ((e = cudaMemcpyAsync(bad_h.data(), cur, static_cast<std::size_t>(n) * sizeof(int),
-                             cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-      return CudaFail(e, "verification readback");
-    }
-    int status = 0;
-    cudaMemcpy(&status, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost);
-    if (status != 0) {
-      cudaMemset(status_.ptr, 0, sizeof(int));
-      return Fail(RDB_E_DEVICE, "segmented walk reported status " + std::to_string(status));
+    if (checked == issued) return drain(RDB_E_DEVICE, "segmented walk did not converge within the pass limit");
+    const int k = checked % kDepth;
+    if ((e = cudaEventSynchronize(pass_ev_[k])) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "pass wait"));
+    const int* slot = ring_h_ + static_cast<std::size_t>(k) * slot_ints;
+    if (slot[n] != 0) {
+      return drain(RDB_E_DEVICE, "segmented walk reported status " + std::to_string(slot[n]));
     }
     if (profiling_) {
       float ms = 0.0f;
-      cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+      cudaEventElapsedTime(&ms, walk_ev_[2 * k], walk_ev_[2 * k + 1]);
       stats_.walk_ms += ms;
       stats_.walk_launches += 1;
       stats_.passes += 1;
-      stats_.launches += 1 + 1 + (use_cache ? 2 : 0);  // walk, segment check, [prepare, key check]
       for (int i = 0; i < n; ++i) {
         const TswImage& im = imgs[static_cast<std::size_t>(i)];
         const int f0 = std::max(front[static_cast<std::size_t>(i)], 0);
         if (f0 >= im.nsegs) continue;
         stats_.walk_positions += im.n - static_cast<int64_t>(f0) * seg_len;
-        if (pass == 0) {
-          for (int k = std::max(f0, 1); k < im.nsegs; ++k) {
-            stats_.walk_positions += std::min(k * seg_len, warm_len);
+        if (checked == 0) {
+          for (int kk = std::max(f0, 1); kk < im.nsegs; ++kk) {
+            stats_.walk_positions += std::min(kk * seg_len, warm_len);
           }
         }
       }
@@ -1051,18 +1131,19 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     // The verified prefix of every unfinished image grows by at least one
     // segment a pass (its first walked segment started from exact state);
     // anything else is an engine fault, reported rather than looped on.
-    bool done = true;
+    done = true;
     for (int i = 0; i < n; ++i) {
       const std::size_t si = static_cast<std::size_t>(i);
-      const int nf = std::min(bad_h[si], imgs[si].nsegs);
+      const int nf = std::min(slot[i], imgs[si].nsegs);
       if (nf < imgs[si].nsegs && nf <= front[si]) {
-        return Fail(RDB_E_DEVICE, "segmented walk made no progress on an image");
+        return drain(RDB_E_DEVICE, "segmented walk made no progress on an image");
       }
       front[si] = nf;
       done = done && nf >= imgs[si].nsegs;
     }
-    if (done) break;
+    ++checked;
   }
+  const int pass = checked - 1;
   last_passes_ = pass + 1;
   if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
   if (profiling_) {

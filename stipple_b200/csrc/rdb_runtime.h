@@ -23,6 +23,7 @@ const char* LastError();
 std::size_t BytesPerPixel(int layout);
 int Fail(int code, const std::string& msg);
 int CudaFail(cudaError_t e, const char* what);
+std::string CudaErr(cudaError_t e, const char* what);
 
 // A device buffer that only grows.
 struct DevBuf {
@@ -137,6 +138,16 @@ class Context {
   bool profiling_ = false;
   rdb_kernel_stats stats_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};
+  // Pipelined pass loop of the segmented walk: a pinned ring of per-pass
+  // results and the events that mark each pass done (and time its walk).
+  int PinnedRing(std::size_t ints);
+  int PassEvents(int depth);
+  int* ring_h_ = nullptr;
+  std::size_t ring_cap_ = 0;
+  std::vector<cudaEvent_t> pass_ev_;
+  cudaEvent_t scratch_ev_ = nullptr;   // end of the last call's work (scratch reuse)
+  cudaStream_t scratch_stream_ = nullptr;
+  std::vector<cudaEvent_t> walk_ev_;
 
  public:
   int last_passes() const { return last_passes_; }

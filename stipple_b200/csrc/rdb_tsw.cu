@@ -376,6 +376,9 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
   if (k >= im.nsegs) return;
   const int front = front_of(L, lo, im.nsegs);
   if (k < front) return;  // verified earlier, not walked
+  // Only the image's FIRST failure matters: segments past one already found
+  // need no check.  (A relaxed read; a stale value only costs a check.)
+  if (k > *reinterpret_cast<volatile const int*>(L.bad[L.pass & 1] + lo)) return;
   bool ok = true;
   if (k > front) {
     // The first walked segment started from a verified predecessor's queue.
