@@ -907,25 +907,16 @@ int Context::SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cuda
 }
 
 // Automatic sequential mode: short images walk whole on one warp each, long
-// ones are segmented -- on thread walkers unless the palette associates alpha.
+// ones are segmented on thread walkers.
 int Context::SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
-  std::vector<rdb_job> plain, warp, thread;
+  std::vector<rdb_job> plain, thread;
   for (int i = 0; i < n; ++i) {
     const rdb_job& j = jobs[i];
     const int64_t px = int64_t{j.width} * j.height;
-    if (px < 8192) {
-      plain.push_back(j);
-    } else if (Plan(j.palette_id)->assoc) {
-      warp.push_back(j);
-    } else {
-      thread.push_back(j);
-    }
+    (px < 8192 ? plain : thread).push_back(j);
   }
   if (!plain.empty()) {
     if (int rc = Seq(plain.data(), static_cast<int>(plain.size()), o, s)) return rc;
-  }
-  if (!warp.empty()) {
-    if (int rc = SeqSegmented(warp.data(), static_cast<int>(warp.size()), o, s)) return rc;
   }
   if (!thread.empty()) {
     if (int rc = SeqThreadSegmented(thread.data(), static_cast<int>(thread.size()), o, s)) return rc;
@@ -937,6 +928,17 @@ int Context::SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStrea
 // cut into segments of seg_len positions, one thread each; passes repeat
 // until each image's verified prefix covers it.
 int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  // One launch walks palettes of one kind: three channels and direct key maps
+  // without alpha, four channels and hashed maps with it.
+  {
+    std::vector<rdb_job> rgb, alpha;
+    for (int i = 0; i < n; ++i) (Plan(jobs[i].palette_id)->assoc ? alpha : rgb).push_back(jobs[i]);
+    if (!rgb.empty() && !alpha.empty()) {
+      if (int rc = SeqThreadSegmented(rgb.data(), static_cast<int>(rgb.size()), o, s)) return rc;
+      return SeqThreadSegmented(alpha.data(), static_cast<int>(alpha.size()), o, s);
+    }
+  }
+  const bool assoc = Plan(jobs[0].palette_id)->assoc;
   const bool use_cache = o.use_cache != 0;
   const int warm_len = std::max(16, o.warm_len > 0 ? o.warm_len : 64);
   constexpr int kChunk = 128;
@@ -950,7 +952,6 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   int64_t all_px = 0;
   for (int i = 0; i < n; ++i) {
     const DevPlan* p = Plan(jobs[i].palette_id);
-    if (p->assoc) return Fail(RDB_E_UNSUPPORTED, "thread segmented walk: alpha-associated palette");
     plan_max = std::max(plan_max, p->smem);
     all_px += int64_t{jobs[i].width} * jobs[i].height;
   }
@@ -961,7 +962,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   // every segment of the call on a resident thread -- one wave per pass.
   int seg_len = o.seg_len;
   if (seg_len <= 0) {
-    const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_));
+    const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0));
     seg_len = static_cast<int>(std::min<int64_t>(1024, (all_px + resident - 1) / resident));
   }
   seg_len = (std::max(seg_len, 64) + 15) & ~15;
@@ -983,7 +984,9 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     im.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
     im.plan = p->dev;
     im.plan_smem = p->smem;
-    if (int rc = Uniform(j.palette_id, s, &im.uni)) return rc;
+    if (!assoc) {
+      if (int rc = Uniform(j.palette_id, s, &im.uni)) return rc;
+    }
     im.first_seg = total;
     im.nsegs = (im.n + seg_len - 1) / seg_len;
     im.cx_offset = positions;
@@ -998,7 +1001,25 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   while ((1 << own_bits) < 2 * seg_len) ++own_bits;
   const std::size_t own_entries = static_cast<std::size_t>(total) << own_bits;
   const std::size_t q_bytes = static_cast<std::size_t>(total) * 64 * sizeof(double);
-  const std::size_t g_words = static_cast<std::size_t>(n) * 3 * kKeys;
+  // Key maps: direct (3 x 2^18 words per image) without alpha; with alpha a
+  // hashed map per image of 4 x n slots (at least 4096, at most 2^25 -- twice
+  // the 2^24 possible keys): keys, two first-touch words, usemin, slot list.
+  std::vector<uint32_t> hcap(static_cast<std::size_t>(n), 0);
+  std::vector<std::size_t> g_off(static_cast<std::size_t>(n), 0);
+  std::size_t g_words = 0;
+  for (int i = 0; i < n; ++i) {
+    const std::size_t si = static_cast<std::size_t>(i);
+    g_off[si] = g_words;
+    if (assoc) {
+      uint32_t cap = 4096;
+      const int64_t want = 4 * int64_t{jobs[i].width} * jobs[i].height;
+      while (static_cast<int64_t>(cap) < want && cap < (1u << 25)) cap <<= 1;
+      hcap[si] = cap;
+      g_words += 5 * static_cast<std::size_t>(cap) + 4;
+    } else {
+      g_words += 3 * static_cast<std::size_t>(kKeys);
+    }
+  }
   if (int rc = Reserve(&tsw_images_, imgs.size() * sizeof(TswImage), "segmented walk images")) return rc;
   if (int rc = Reserve(&tsw_chunks_, chunks.size() * sizeof(TswChunk), "segment chunks")) return rc;
   if (int rc = Reserve(&tsw_bad_, 2 * static_cast<std::size_t>(n) * sizeof(int), "verification flags")) return rc;
@@ -1012,11 +1033,19 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     if (int rc = Reserve(&tsw_g_, g_words * sizeof(uint32_t), "first-touch maps")) return rc;
     uint32_t* g = static_cast<uint32_t*>(tsw_g_.ptr);
     for (int i = 0; i < n; ++i) {
-      TswImage& im = imgs[static_cast<std::size_t>(i)];
-      uint32_t* base = g + static_cast<std::size_t>(i) * 3 * kKeys;
+      const std::size_t si = static_cast<std::size_t>(i);
+      TswImage& im = imgs[si];
+      uint32_t* base = g + g_off[si];
+      const std::size_t cap = assoc ? hcap[si] : static_cast<std::size_t>(kKeys);
       im.g[0] = base;
-      im.g[1] = base + kKeys;
-      im.usemin = base + 2 * static_cast<std::size_t>(kKeys);
+      im.g[1] = base + cap;
+      im.usemin = base + 2 * cap;
+      if (assoc) {
+        im.hkeys = base + 3 * cap;
+        im.hlist = base + 4 * cap;
+        im.hcount = reinterpret_cast<int*>(base + 5 * cap);
+        im.hmask = hcap[si] - 1;
+      }
     }
   }
   cudaError_t e;
@@ -1045,6 +1074,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.chosen = static_cast<uint8_t*>(tsw_chosen_.ptr);
   L.use_cache = use_cache ? 1 : 0;
   L.is_float = is_float ? 1 : 0;
+  L.assoc = assoc ? 1 : 0;
   L.plan_smem_max = plan_max;
   L.chunk_threads = kChunk;
   L.bad[0] = bad;
@@ -1057,7 +1087,16 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   if (use_cache) {
     cudaMemsetAsync(tsw_own_.ptr, 0, own_entries * sizeof(uint64_t), s);
     for (int i = 0; i < n; ++i) {
-      cudaMemsetAsync(imgs[static_cast<std::size_t>(i)].g[1], 0xFF, kKeys * sizeof(uint32_t), s);
+      const TswImage& im = imgs[static_cast<std::size_t>(i)];
+      if (assoc) {
+        // Empty keys and counts; every first-touch and usemin word "none".
+        const std::size_t cap = hcap[static_cast<std::size_t>(i)];
+        cudaMemsetAsync(im.g[0], 0xFF, 3 * cap * sizeof(uint32_t), s);
+        cudaMemsetAsync(im.hkeys, 0, cap * sizeof(uint32_t), s);
+        cudaMemsetAsync(im.hcount, 0, sizeof(int), s);
+      } else {
+        cudaMemsetAsync(im.g[1], 0xFF, kKeys * sizeof(uint32_t), s);
+      }
     }
   }
   if ((e = LaunchTswGather(L, positions, s)) != cudaSuccess) return CudaFail(e, "sample gather");

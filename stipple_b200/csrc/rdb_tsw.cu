@@ -17,7 +17,7 @@ namespace rdb {
 namespace {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
-constexpr uint32_t kNoUser = 0x7FFFFFFFu;
+constexpr uint32_t kNoUser = 0xFFFFFFFFu;
 constexpr int kKeys = 1 << 18;
 
 __device__ __forceinline__ int front_of(const TswLaunch& L, int image, int nsegs) {
@@ -66,37 +66,53 @@ __global__ void TswGather(TswLaunch L, int64_t total) {
   }
 }
 
-template <bool kFloat>
-__device__ __forceinline__ void sample(const TswLaunch& L, int64_t at, double (&p)[3]) {
+// One curve position's sample as the walk sees it (AssociateAlphaPixel,
+// rd_types.h:179-192, when the palette associates alpha).
+template <bool kFloat, int C>
+__device__ __forceinline__ void sample(const TswLaunch& L, int64_t at, double (&p)[C]) {
   if (kFloat) {
     const float4 s = reinterpret_cast<const float4*>(L.cx)[at];
-    p[0] = static_cast<double>(s.x);
-    p[1] = static_cast<double>(s.y);
-    p[2] = static_cast<double>(s.z);
+    double a4[4];
+    associate_sample(C == 4, s, a4[0], a4[1], a4[2], a4[3]);
+#pragma unroll
+    for (int c = 0; c < C; ++c) p[c] = a4[c];
   } else {
     const uint32_t w = reinterpret_cast<const uint32_t*>(L.cx)[at];
-    p[0] = static_cast<double>((w & 0xFFu) * 257u);
-    p[1] = static_cast<double>(((w >> 8) & 0xFFu) * 257u);
-    p[2] = static_cast<double>(((w >> 16) & 0xFFu) * 257u);
+    const double r = static_cast<double>((w & 0xFFu) * 257u);
+    const double g = static_cast<double>(((w >> 8) & 0xFFu) * 257u);
+    const double b = static_cast<double>(((w >> 16) & 0xFFu) * 257u);
+    p[0] = r;
+    p[1] = g;
+    p[2] = b;
+    if constexpr (C == 4) {
+      const unsigned a8 = w >> 24;
+      p[3] = static_cast<double>(a8 * 257u);
+      if (a8 != 255u) {
+        const double alpha = __dmul_rn(kQuantumScale, p[3]);
+        p[0] = __dmul_rn(alpha, r);
+        p[1] = __dmul_rn(alpha, g);
+        p[2] = __dmul_rn(alpha, b);
+      }
+    }
   }
 }
 
 // Pixel t (slot U) takes its last term w15 * e_{t-1}; the 15 pixels after it
 // take e_{t-1} with their weights; slot U is refilled with pixel t + 16.
-template <int U>
-__device__ __forceinline__ void Rotate(const double (&sw)[16], double (&R)[16][3],
-                                       const double (&e)[3], double (&v)[3], const double (&p)[3]) {
+template <int U, int C>
+__device__ __forceinline__ void Rotate(const double (&sw)[16], double (&R)[16][C],
+                                       const double (&e)[C], double (&v)[C], const double (&p)[C]) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) v[c] = __dadd_rn(R[U][c], __dmul_rn(sw[15], e[c]));
+  for (int c = 0; c < C; ++c) v[c] = __dadd_rn(R[U][c], __dmul_rn(sw[15], e[c]));
 #pragma unroll
   for (int jj = 1; jj < 16; ++jj) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < C; ++c) {
       R[(U + jj) & 15][c] = __dadd_rn(R[(U + jj) & 15][c], __dmul_rn(sw[15 - jj], e[c]));
     }
   }
 #pragma unroll
-  for (int c = 0; c < 3; ++c) R[U][c] = p[c];
+  for (int c = 0; c < C; ++c) R[U][c] = p[c];
 }
 
 __device__ __forceinline__ unsigned own_hash(unsigned key) { return (key * 0x9E3779B1u) >> 8; }
@@ -106,15 +122,65 @@ __device__ __forceinline__ void red_min(uint32_t* p, uint32_t v) {
   asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// ---- hashed key maps (alpha keys: 24 bits) ----------------------------------
+// keys[slot] = key + 1 (0 = empty), inserted with atomicCAS and never removed;
+// every inserted slot is appended to the image's slot list, which the per-key
+// kernels walk instead of the whole table.
+__device__ __forceinline__ unsigned map_hash(unsigned key) { return key * 0x9E3779B1u; }
+
+// The key's slot (present) or the first empty slot of its probe run (absent);
+// -1 when the table is full.  Keys are read plainly: an insert by another
+// thread that is not yet visible only sends this one to insert, where the CAS
+// sees it.
+__device__ __forceinline__ int map_find(const uint32_t* keys, uint32_t mask, unsigned key,
+                                        bool* present) {
+  unsigned h = map_hash(key) & mask;
+#pragma unroll 1
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const uint32_t k1 = reinterpret_cast<const volatile uint32_t*>(keys)[h];
+    if (k1 == key + 1u) {
+      *present = true;
+      return static_cast<int>(h);
+    }
+    if (k1 == 0u) {
+      *present = false;
+      return static_cast<int>(h);
+    }
+    h = (h + 1u) & mask;
+  }
+  *present = false;
+  return -1;
+}
+
+__device__ __forceinline__ int map_insert(uint32_t* keys, uint32_t mask, unsigned key, int from,
+                                          uint32_t* list, int* count) {
+  if (from < 0) return -1;
+  unsigned h = static_cast<unsigned>(from);
+#pragma unroll 1
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const uint32_t old = atomicCAS(keys + h, 0u, key + 1u);
+    if (old == 0u) {
+      list[atomicAdd(count, 1)] = h;
+      return static_cast<int>(h);
+    }
+    if (old == key + 1u) return static_cast<int>(h);
+    h = (h + 1u) & mask;
+  }
+  return -1;
+}
+
 // Segment k of one image, one thread per segment.  The step loop is
 // warp-uniform (every lane runs the warp's longest segment's step count,
 // idle past its own), so lanes that need a colour search hand it to the
 // whole warp: each search is spread over the 32 lanes instead of running
-// serially in one lane while the other 31 wait.
-template <bool kFloat>
+// serially in one lane while the other 31 wait.  kAssoc: the palette
+// associates alpha (four channels, 24-bit keys in hashed maps, no
+// uniform-key table); otherwise three channels and direct 2^18-key maps.
+template <bool kFloat, bool kAssoc>
 __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& im,
                                             const tw::Plan& P, const double* errp, int k,
                                             bool active, int lane) {
+  constexpr int C = kAssoc ? 4 : 3;
   const int sid = im.first_seg + k;
   const int begin = k * L.seg_len;
   const int end = active ? min(begin + L.seg_len, im.n) : begin;
@@ -124,14 +190,18 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   const int64_t base = im.cx_offset;
   const bool memo = L.use_cache != 0;
 
-  double R[16][3];
-  double e[3] = {0.0, 0.0, 0.0};
+  double R[16][C];
+  double e[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) e[c] = 0.0;
 #pragma unroll
   for (int u = 0; u < 16; ++u) {
-    double p[3] = {0.0, 0.0, 0.0};
-    if (ws + u < end) sample<kFloat>(L, base + ws + u, p);
+    double p[C];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) R[u][c] = p[c];
+    for (int c = 0; c < C; ++c) p[c] = 0.0;
+    if (ws + u < end) sample<kFloat, C>(L, base + ws + u, p);
+#pragma unroll
+    for (int c = 0; c < C; ++c) R[u][c] = p[c];
   }
   if (active && !warmup && k > 0) {
     // Start from the predecessor's end queue q[0..15] (oldest first): pixel
@@ -140,17 +210,17 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     const double* q = L.q_end[(L.pass & 1) ^ 1] + static_cast<int64_t>(sid - 1) * 64;
 #pragma unroll
     for (int m = 0; m < 15; ++m) {
-      double qm[3];
+      double qm[C];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) qm[c] = q[4 * m + c];
+      for (int c = 0; c < C; ++c) qm[c] = q[4 * m + c];
 #pragma unroll
       for (int j = 0; j <= m; ++j) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) R[j][c] = __dadd_rn(R[j][c], __dmul_rn(L.sw[m - j], qm[c]));
+        for (int c = 0; c < C; ++c) R[j][c] = __dadd_rn(R[j][c], __dmul_rn(L.sw[m - j], qm[c]));
       }
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) e[c] = q[60 + c];
+    for (int c = 0; c < C; ++c) e[c] = q[60 + c];
   }
 
   const uint32_t* gprev = im.g[(L.pass & 1) ^ 1];
@@ -164,6 +234,8 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   uint8_t* out = L.chosen + base;
   const uint8_t* uni = im.uni;
   uint32_t* usemin = im.usemin;
+  uint32_t* hkeys = im.hkeys;
+  const uint32_t hmask = im.hmask;
   const int warp_steps = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(steps));
   int n_own = 0;
   uint32_t acc = 0;
@@ -172,44 +244,60 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     const bool on = i < steps;
     const int t = ws + i;
     const int u = i & 15;
-    float f[3] = {0.0f, 0.0f, 0.0f};
-    unsigned br = 0, bg = 0, bb = 0, key = 0, h = 0;
-    int index = 0;
-    bool search = false, record = false, from_g = false, booked = false;
+    float f[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    unsigned br = 0, bg = 0, bb = 0, ba = 0, key = 0, h = 0;
+    int index = 0, slot = 0;
+    bool search = false, record = false, from_g = false, booked = false, present = true;
     const bool live = t >= begin;
     const bool keyed = on && memo && live;
     if (on) {
-      double p[3] = {0.0, 0.0, 0.0};
-      if (t + 16 < end) sample<kFloat>(L, base + t + 16, p);
-      double v[3];
+      double p[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) p[c] = 0.0;
+      if (t + 16 < end) sample<kFloat, C>(L, base + t + 16, p);
+      double v[C];
       switch (u) {
-        case 0: Rotate<0>(L.sw, R, e, v, p); break;
-        case 1: Rotate<1>(L.sw, R, e, v, p); break;
-        case 2: Rotate<2>(L.sw, R, e, v, p); break;
-        case 3: Rotate<3>(L.sw, R, e, v, p); break;
-        case 4: Rotate<4>(L.sw, R, e, v, p); break;
-        case 5: Rotate<5>(L.sw, R, e, v, p); break;
-        case 6: Rotate<6>(L.sw, R, e, v, p); break;
-        case 7: Rotate<7>(L.sw, R, e, v, p); break;
-        case 8: Rotate<8>(L.sw, R, e, v, p); break;
-        case 9: Rotate<9>(L.sw, R, e, v, p); break;
-        case 10: Rotate<10>(L.sw, R, e, v, p); break;
-        case 11: Rotate<11>(L.sw, R, e, v, p); break;
-        case 12: Rotate<12>(L.sw, R, e, v, p); break;
-        case 13: Rotate<13>(L.sw, R, e, v, p); break;
-        case 14: Rotate<14>(L.sw, R, e, v, p); break;
-        default: Rotate<15>(L.sw, R, e, v, p); break;
+        case 0: Rotate<0, C>(L.sw, R, e, v, p); break;
+        case 1: Rotate<1, C>(L.sw, R, e, v, p); break;
+        case 2: Rotate<2, C>(L.sw, R, e, v, p); break;
+        case 3: Rotate<3, C>(L.sw, R, e, v, p); break;
+        case 4: Rotate<4, C>(L.sw, R, e, v, p); break;
+        case 5: Rotate<5, C>(L.sw, R, e, v, p); break;
+        case 6: Rotate<6, C>(L.sw, R, e, v, p); break;
+        case 7: Rotate<7, C>(L.sw, R, e, v, p); break;
+        case 8: Rotate<8, C>(L.sw, R, e, v, p); break;
+        case 9: Rotate<9, C>(L.sw, R, e, v, p); break;
+        case 10: Rotate<10, C>(L.sw, R, e, v, p); break;
+        case 11: Rotate<11, C>(L.sw, R, e, v, p); break;
+        case 12: Rotate<12, C>(L.sw, R, e, v, p); break;
+        case 13: Rotate<13, C>(L.sw, R, e, v, p); break;
+        case 14: Rotate<14, C>(L.sw, R, e, v, p); break;
+        default: Rotate<15, C>(L.sw, R, e, v, p); break;
       }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) f[c] = clamp_pixel(v[c]);
+      for (int c = 0; c < C; ++c) f[c] = clamp_pixel(v[c]);
       br = byte_dev(f[0]);
       bg = byte_dev(f[1]);
       bb = byte_dev(f[2]);
       key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12);
+      if constexpr (kAssoc) {
+        ba = byte_dev(f[3]);
+        key |= (ba >> 2) << 18;
+      }
       // A uniform key's search result (and so its memo value) is fixed by the
       // key: no search, no memo, no bookkeeping.
-      const uint8_t uv = __ldg(uni + key);
-      const uint32_t gv = keyed ? __ldg(gprev + key) : kNone;  // both loads in flight together
+      uint8_t uv = kNotUniform;
+      uint32_t gv = kNone;
+      if constexpr (kAssoc) {
+        if (keyed) {
+          slot = map_find(hkeys, hmask, key, &present);
+          if (present) gv = __ldg(gprev + slot);
+        }
+      } else {
+        uv = __ldg(uni + key);
+        slot = static_cast<int>(key);
+        if (keyed) gv = __ldg(gprev + key);  // both loads in flight together
+      }
       search = uv == kNotUniform;
       index = uv;
       booked = keyed && search;
@@ -247,27 +335,40 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     }
     // The warp's searches, one target at a time over all 32 lanes.
     unsigned want = __ballot_sync(0xffffffffu, search);
-    const int node = search ? tw::descend<false>(P, br, bg, bb, 0u) : 0;
+    const int node = search ? tw::descend<kAssoc>(P, br, bg, bb, ba) : 0;
 #pragma unroll 1
     while (want) {
       const int src = __ffs(want) - 1;
       want &= want - 1u;
       const int sn = __shfl_sync(0xffffffffu, node, src);
-      const float s0 = __shfl_sync(0xffffffffu, f[0], src);
-      const float s1 = __shfl_sync(0xffffffffu, f[1], src);
-      const float s2 = __shfl_sync(0xffffffffu, f[2], src);
-      const int r = tw::search_warp<false>(P, sn, s0, s1, s2, 0.0, lane);
+      double t4[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) t4[c] = static_cast<double>(__shfl_sync(0xffffffffu, f[c], src));
+      if constexpr (kAssoc) {
+        // ClosestColor's target: beta * t with beta = QS * t.a (rd_octree.cpp:190-208).
+        const double beta = __dmul_rn(kQuantumScale, t4[3]);
+        t4[0] = __dmul_rn(beta, t4[0]);
+        t4[1] = __dmul_rn(beta, t4[1]);
+        t4[2] = __dmul_rn(beta, t4[2]);
+      }
+      const int r = tw::search_warp<kAssoc>(P, sn, t4[0], t4[1], t4[2], t4[3], lane);
       if (lane == src) index = r;
     }
-    if (booked) red_min(gnew + key, (static_cast<uint32_t>(k) << 8) | static_cast<uint32_t>(index));
-    if (from_g) red_min(usemin + key, static_cast<uint32_t>(k));
+    if (booked) {
+      if constexpr (kAssoc) {
+        if (!present) slot = map_insert(hkeys, hmask, key, slot, im.hlist, im.hcount);
+        if (slot < 0) atomicExch(L.status, kDevBadPlan);  // key map full: cannot happen at its size
+      }
+      if (slot >= 0) red_min(gnew + slot, (static_cast<uint32_t>(k) << 8) | static_cast<uint32_t>(index));
+    }
+    if (from_g) red_min(usemin + slot, static_cast<uint32_t>(k));
     if (on) {
       if (record) {
         ot[h] = tag | static_cast<uint64_t>(key) | (static_cast<uint64_t>(index) << 24);
         ol[n_own++] = key | (static_cast<uint32_t>(index) << 24);
       }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) e[c] = __dadd_rn(static_cast<double>(f[c]), -errp[c * kMaxPaletteColors + index]);
+      for (int c = 0; c < C; ++c) e[c] = __dadd_rn(static_cast<double>(f[c]), -errp[c * kMaxPaletteColors + index]);
       if (live) {
         const int q = (t - begin) & 3;
         acc |= static_cast<uint32_t>(index) << (8 * q);
@@ -279,25 +380,21 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
         }
         if (t >= end - 16) {
           double* d = qe + 4 * (t - (end - 16));
-          d[0] = e[0];
-          d[1] = e[1];
-          d[2] = e[2];
-          d[3] = 0.0;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
         }
       } else if (t >= begin - 16) {
         double* d = qs + 4 * (t - (begin - 16));
-        d[0] = e[0];
-        d[1] = e[1];
-        d[2] = e[2];
-        d[3] = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
       }
     }
   }
   if (active && memo) L.own_count[sid] = n_own;
 }
 
-template <bool kFloat>
-__global__ void __launch_bounds__(128, 3) TswWalkKernel(TswLaunch L) {
+template <bool kFloat, bool kAssoc>
+__global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TswChunk ch = L.chunks[blockIdx.x];
   const TswImage& im = L.images[ch.image];
@@ -311,14 +408,15 @@ __global__ void __launch_bounds__(128, 3) TswWalkKernel(TswLaunch L) {
   __syncthreads();
   // Residual-side colours channel-planar (colour i of channel c at
   // c * 256 + i): lanes holding different indices then spread over the banks
-  // instead of meeting in the 32-byte palette rows.
+  // instead of meeting in the palette rows.
+  constexpr int C = kAssoc ? 4 : 3;
   double* errp = reinterpret_cast<double*>(smem + L.plan_smem_max);
   {
     tw::Plan P0;
     P0.bind(smem);
-    for (int i = threadIdx.x; i < 3 * kMaxPaletteColors; i += blockDim.x) {
+    for (int i = threadIdx.x; i < C * kMaxPaletteColors; i += blockDim.x) {
       const int c = i / kMaxPaletteColors, col = i - c * kMaxPaletteColors;
-      errp[i] = col < P0.h->count ? P0.rcol<false>(col)[c] : 0.0;
+      errp[i] = col < P0.h->count ? P0.rcol<kAssoc>(col)[c] : 0.0;
     }
   }
   __syncthreads();
@@ -331,32 +429,43 @@ __global__ void __launch_bounds__(128, 3) TswWalkKernel(TswLaunch L) {
   const bool active = static_cast<int>(threadIdx.x) < ch.count && k >= front;
   tw::Plan P;
   P.bind(smem);
-  WalkSegment<kFloat>(L, im, P, errp, active ? k : warp_end - 1, active, lane);
+  WalkSegment<kFloat, kAssoc>(L, im, P, errp, active ? k : warp_end - 1, active, lane);
 }
 
 // G_new = the entries of G_prev that verified segments made; usemin cleared.
+// Direct maps: one thread per key; hashed maps: the inserted slots.
 __global__ void TswPrepare(TswLaunch L) {
   const int m = blockIdx.y;
-  const int key = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= L.n_images || key >= kKeys) return;
+  if (m >= L.n_images) return;
   const TswImage& im = L.images[m];
   const int front = front_of(L, m, im.nsegs);
-  const uint32_t gv = im.g[(L.pass & 1) ^ 1][key];
-  im.g[L.pass & 1][key] = (gv != kNone && static_cast<int>(gv >> 8) < front) ? gv : kNone;
-  im.usemin[key] = kNoUser;
+  const uint32_t* gp = im.g[(L.pass & 1) ^ 1];
+  uint32_t* gn = im.g[L.pass & 1];
+  const int stride = gridDim.x * blockDim.x;
+  const int n = im.hkeys ? *im.hcount : kKeys;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int slot = im.hkeys ? static_cast<int>(im.hlist[i]) : i;
+    const uint32_t gv = gp[slot];
+    gn[slot] = (gv != kNone && static_cast<int>(gv >> 8) < front) ? gv : kNone;
+    im.usemin[slot] = kNoUser;
+  }
 }
 
 // The "from G" check, per key.
 __global__ void TswVerifyKeys(TswLaunch L) {
   const int m = blockIdx.y;
-  const int key = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= L.n_images || key >= kKeys) return;
+  if (m >= L.n_images) return;
   const TswImage& im = L.images[m];
-  const uint32_t u = im.usemin[key];
-  if (u == kNoUser) return;
-  const uint32_t gp = im.g[(L.pass & 1) ^ 1][key];
-  const uint32_t gn = im.g[L.pass & 1][key];
-  if ((gn & 0xFFu) != (gp & 0xFFu) || (gn >> 8) >= u) atomicMin(L.bad[L.pass & 1] + m, static_cast<int>(u));
+  const int stride = gridDim.x * blockDim.x;
+  const int n = im.hkeys ? *im.hcount : kKeys;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int slot = im.hkeys ? static_cast<int>(im.hlist[i]) : i;
+    const uint32_t u = im.usemin[slot];
+    if (u == kNoUser) continue;
+    const uint32_t gp = im.g[(L.pass & 1) ^ 1][slot];
+    const uint32_t gn = im.g[L.pass & 1][slot];
+    if ((gn & 0xFFu) != (gp & 0xFFu) || (gn >> 8) >= u) atomicMin(L.bad[L.pass & 1] + m, static_cast<int>(u));
+  }
 }
 
 // The queue and own checks, one warp per walked segment.
@@ -395,7 +504,15 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
     const int cnt = L.own_count[sid];
     for (int i = lane; i < cnt; i += 32) {
       const uint32_t w = ol[i];
-      const uint32_t g = gn[w & 0xFFFFFFu];
+      const unsigned key = w & 0xFFFFFFu;
+      uint32_t g = kNone;
+      if (im.hkeys) {
+        bool present = false;
+        const int slot = map_find(im.hkeys, im.hmask, key, &present);
+        if (present) g = gn[slot];
+      } else {
+        g = gn[key];
+      }
       if (static_cast<int>(g >> 8) < k && (g & 0xFFu) != (w >> 24)) ok = false;
     }
   }
@@ -416,27 +533,35 @@ __global__ void TswScatter(TswLaunch L, int64_t total) {
   if (im.rgba_out) {
     const PlanHeader* h = reinterpret_cast<const PlanHeader*>(im.plan);
     const float4 pc = reinterpret_cast<const float4*>(im.plan + h->off_out)[index];
-    const float a = load_sample(im.pixels, im.layout, im.row_stride, im.width, pix).w;
+    const float a = h->assoc ? pc.w : load_sample(im.pixels, im.layout, im.row_stride, im.width, pix).w;
     im.rgba_out[pix] = make_float4(pc.x, pc.y, pc.z, a);
   }
+}
+
+template <bool kFloat, bool kAssoc>
+cudaError_t LaunchWalk(const TswLaunch& L, int smem, cudaStream_t s) {
+  const cudaError_t e = AllowMaxSmem(TswWalkKernel<kFloat, kAssoc>);
+  if (e != cudaSuccess) return e;
+  TswWalkKernel<kFloat, kAssoc><<<L.n_chunks, L.chunk_threads, smem, s>>>(L);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
 std::size_t TswSmemBytes(int plan_smem_max) {
-  return static_cast<std::size_t>(plan_smem_max) + 3 * kMaxPaletteColors * sizeof(double);
+  return static_cast<std::size_t>(plan_smem_max) + 4 * kMaxPaletteColors * sizeof(double);
 }
 
-int TswResidentThreads(int plan_smem_max, int sm_count) {
+int TswResidentThreads(int plan_smem_max, int sm_count, int assoc) {
   const int smem = static_cast<int>(TswSmemBytes(plan_smem_max));
-  if (AllowMaxSmem(TswWalkKernel<false>) != cudaSuccess) {
-    return 0;
-  }
-  int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, TswWalkKernel<false>, 128, smem) !=
+  const void* k = assoc ? reinterpret_cast<const void*>(TswWalkKernel<false, true>)
+                        : reinterpret_cast<const void*>(TswWalkKernel<false, false>);
+  if ((assoc ? AllowMaxSmem(TswWalkKernel<false, true>) : AllowMaxSmem(TswWalkKernel<false, false>)) !=
       cudaSuccess) {
     return 0;
   }
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, 128, smem) != cudaSuccess) return 0;
   return blocks * 128 * sm_count;
 }
 
@@ -455,17 +580,8 @@ cudaError_t LaunchTswPrepare(const TswLaunch& L, cudaStream_t s) {
 cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s) {
   if (L.n_chunks <= 0) return cudaSuccess;
   const int smem = static_cast<int>(TswSmemBytes(L.plan_smem_max));
-  cudaError_t e;
-  if (L.is_float) {
-    e = AllowMaxSmem(TswWalkKernel<true>);
-    if (e != cudaSuccess) return e;
-    TswWalkKernel<true><<<L.n_chunks, L.chunk_threads, smem, s>>>(L);
-  } else {
-    e = AllowMaxSmem(TswWalkKernel<false>);
-    if (e != cudaSuccess) return e;
-    TswWalkKernel<false><<<L.n_chunks, L.chunk_threads, smem, s>>>(L);
-  }
-  return cudaGetLastError();
+  if (L.assoc) return L.is_float ? LaunchWalk<true, true>(L, smem, s) : LaunchWalk<false, true>(L, smem, s);
+  return L.is_float ? LaunchWalk<true, false>(L, smem, s) : LaunchWalk<false, false>(L, smem, s);
 }
 
 cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) {

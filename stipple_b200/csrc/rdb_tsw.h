@@ -1,5 +1,5 @@
 // rdb_tsw.h -- the speculative segmented walk on thread walkers: one thread
-// per segment, for palettes without associated alpha.
+// per segment.
 //
 // The exactness argument is the one of rdb_ssw.h (segments replayed from
 // guessed states, checked against their predecessors, a verified prefix that
@@ -52,8 +52,17 @@ struct TswImage {
   int first_seg;             // global id of segment 0
   int nsegs;
   int64_t cx_offset;         // first position in the gathered sample / index buffers
-  uint32_t* g[2];            // first-touch maps (2^18 entries each); pass p writes g[p & 1]
-  uint32_t* usemin;          // 2^18: earliest segment that took the key from G_prev
+  uint32_t* g[2];            // first-touch maps; pass p writes g[p & 1]
+  uint32_t* usemin;          // earliest segment that took the key from G_prev
+  // Direct maps (no alpha): g and usemin have 2^18 entries indexed by key and
+  // hkeys is null.  Hashed maps (alpha keys, 24 bits): hmask + 1 slots,
+  // hkeys[slot] = key + 1 (0 = empty), every inserted slot listed in
+  // hlist[0 .. *hcount).
+  uint32_t* hkeys;
+  uint32_t* hlist;
+  int* hcount;
+  uint32_t hmask;
+  int pad2;
 };
 
 // A CTA's work: segments k0 .. k0 + count - 1 of one image (one plan per CTA).
@@ -83,6 +92,7 @@ struct TswLaunch {
   uint8_t* chosen;           // per position
   int use_cache;
   int is_float;
+  int assoc;                 // every palette of the launch associates alpha (or none does)
   int plan_smem_max;
   int chunk_threads;
   // Per image, by pass parity: the first failing segment of that pass (large
@@ -95,7 +105,7 @@ struct TswLaunch {
 
 std::size_t TswSmemBytes(int plan_smem_max);
 // Walker threads the device holds at once (0 if the query fails).
-int TswResidentThreads(int plan_smem_max, int sm_count);
+int TswResidentThreads(int plan_smem_max, int sm_count, int assoc);
 // Samples of every image in visit order, into L.cx.
 cudaError_t LaunchTswGather(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
 // G_new = verified entries of G_prev, usemin cleared (memo only).

@@ -111,12 +111,60 @@ def test_thread_segmented_full_hd_auto(ctx, oracle):
         ctx.release_palette(pid)
 
 
-def test_thread_segmented_refuses_alpha_palette(ctx):
-    img = synth.gradient_rgba8(128, 96, 3)
-    t = sb.Octree(img, 16, True)
-    pid = ctx.palette_from_octree(t)
+@pytest.mark.parametrize("seg,warm", [(64, 16), (256, 64)])
+def test_thread_segmented_alpha(ctx, oracle, seg, warm):
+    """Alpha-associated palettes: four channels, 24-bit keys in hashed maps."""
+    for k, (w, h, colors) in enumerate([(256, 192, 16), (300, 211, 256), (97, 403, 4), (640, 64, 64)]):
+        img = synth.gradient_rgba8(w, h, 60 + k)
+        t = sb.Octree(img, colors, True)
+        pid = ctx.palette_from_octree(t)
+        try:
+            got, rgba = ctx.dither_host("seq", img, pid, rgba=True, seq_mode=3, seg_len=seg,
+                                        warm_len=warm)
+            want, out, _ = oracle.walk_seq(synth.to_q16(img), colors, True, t.grayscale)
+            assert np.array_equal(got, want), (w, h, colors, seg, warm)
+            assert np.array_equal(rgba.view(np.uint32), out.view(np.uint32)), (w, h, colors)
+        finally:
+            ctx.release_palette(pid)
+
+
+def test_thread_segmented_alpha_float_and_no_cache(ctx, oracle):
+    rng = np.random.default_rng(5)
+    q = (rng.random((120, 170, 4)) * 65535.0).astype(np.float32)
+    q[..., 3] = np.where(rng.random((120, 170)) < 0.3, q[..., 3], 65535.0)
+    tree = oracle.build_tree(q, 64, True, False)
+    pid = ctx.palette(tree.palette, tree.child, tree.color_number, tree.number_unique, True,
+                      parent=tree.parent)
     try:
-        with pytest.raises(sb.RdbError):
-            ctx.dither_host("seq", img, pid, seq_mode=3)
+        for cache in (1, 0):
+            got = ctx.dither_host("seq", q, pid, seq_mode=3, seg_len=128, warm_len=32,
+                                  use_cache=cache)
+            want, _, _ = oracle.walk_seq(q, 64, True, False, use_cache=bool(cache))
+            assert np.array_equal(got, want), cache
     finally:
         ctx.release_palette(pid)
+
+
+def test_thread_segmented_mixed_alpha_batch(ctx, oracle):
+    """A batch mixing alpha and plain palettes (split into one launch of each
+    kind), every image equal to the oracle."""
+    sizes = [(200, 100), (130, 140), (512, 64), (90, 300), (256, 256)]
+    imgs, pids, want = [], [], []
+    for k, (w, h) in enumerate(sizes):
+        alpha = k % 2 == 0
+        img = synth.gradient_rgba8(w, h, 80 + k) if alpha else synth.gradient_rgb8(w, h, 80 + k)
+        colors = [256, 16, 64, 8, 128][k]
+        t = sb.Octree(img, colors, alpha)
+        pids.append(ctx.palette_from_octree(t))
+        imgs.append(img)
+        want.append(oracle.walk_seq(synth.to_q16(img), colors, alpha, t.grayscale)[0])
+    try:
+        got = ctx.dither_host("seq", imgs, pids, seq_mode=3, seg_len=96, warm_len=32)
+        for k in range(len(imgs)):
+            assert np.array_equal(got[k], want[k]), sizes[k]
+        auto = ctx.dither_host("seq", imgs, pids)
+        for k in range(len(imgs)):
+            assert np.array_equal(auto[k], want[k]), sizes[k]
+    finally:
+        for p in pids:
+            ctx.release_palette(p)
