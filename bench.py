@@ -50,7 +50,7 @@ def parse():
                     help="requests in the served-stream sample (the full stream is 10,000)")
     ap.add_argument("--serve-rates", default="20,60",
                     help="Poisson arrival rates (requests/s) of the served-stream sample")
-    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "blocks"],
+    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "seq_alpha", "blocks", "batched"],
                     help="run only that workload's device steps (for ncu captures) and print "
                          "its timing; no JSON contract line")
     return ap.parse_args()
@@ -238,8 +238,8 @@ def run_ours(a, rank: int, world: int):
     pos_per_launch = kstats["walk_positions"] / launches
     achieved = pos_per_launch * 10 / (walk_ms / 1e3) / 1e9 if walk_ms > 0 else 0.0
     # DRAM bytes of one walk launch of this workload from ncu (dram__bytes_read
-    # + dram__bytes_write, pass 31), profiles/tsw_walk_4k_rgb8_256c.md.
-    traffic = 63954432 + 5931776
+    # + dram__bytes_write, pass 30), profiles/tsw_walk_4k_rgb8_256c.md.
+    traffic = 64074496 + 4203008
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "TswWalkKernel", "walk_ms_per_launch": walk_ms,
@@ -456,10 +456,28 @@ def profile_case(a):
     W, H, C = HEADLINE["width"], HEADLINE["height"], HEADLINE["colors"]
     img = synth.gradient_rgb8(W, H, HEADLINE["seed"])
     pid = ctx.palette_from_octree(sb.Octree(img, C, False, False))
-    if a.profile_case == "seq":
+    if a.profile_case == "batched":
+        rng = np.random.default_rng(5)
+        sizes = synth.log_uniform_sizes(a.batch - 4, seed=2024) + [(1, 1), (3, 5), (17, 13), (4096, 64)]
+        keep, jobs = [], []
+        for k, (w, h) in enumerate(sizes):
+            im = synth.gradient_rgba8(w, h, 1000 + k)
+            p = ctx.palette_from_image(im, int(rng.choice([2, 4, 8, 16, 64, 256])), associate_alpha=True)
+            d = torch.from_numpy(im).cuda()
+            o = torch.empty((h, w), dtype=torch.uint8, device="cuda")
+            keep += [d, o]
+            jobs.append(dict(pixels=d.data_ptr(), width=w, height=h, layout=sb.RGBA8, palette_id=p,
+                             indices=o.data_ptr()))
+        opts = {}
+    elif a.profile_case in ("seq", "seq_alpha"):
+        lay = sb.RGB8
+        if a.profile_case == "seq_alpha":
+            img = synth.gradient_rgba8(W, H, HEADLINE["seed"])
+            pid = ctx.palette_from_image(img, C, associate_alpha=True)
+            lay = sb.RGBA8
         d = torch.from_numpy(img).cuda()
         o = torch.empty((H, W), dtype=torch.uint8, device="cuda")
-        jobs = [dict(pixels=d.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
+        jobs = [dict(pixels=d.data_ptr(), width=W, height=H, layout=lay, palette_id=pid,
                      indices=o.data_ptr())]
         opts = {}
     else:
@@ -469,7 +487,7 @@ def profile_case(a):
         jobs = [dict(pixels=f.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
                      indices=x.data_ptr()) for f, x in zip(frames, outs)]
         opts = {"block": 256}
-    engine = "seq" if a.profile_case == "seq" else "blocks"
+    engine = "blocks" if a.profile_case == "blocks" else "seq"
     for _ in range(a.warmup):
         ctx.dither(engine, jobs, stream=s, **opts)
     ctx.synchronize(s)
