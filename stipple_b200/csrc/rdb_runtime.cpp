@@ -64,6 +64,9 @@ Context::~Context() {
     if (ev) cudaEventDestroy(ev);
   }
   for (cudaEvent_t ev : pass_ev_) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : tune_ev_) {
+    if (ev) cudaEventDestroy(ev);
+  }
   if (scratch_ev_) cudaEventDestroy(scratch_ev_);
   for (cudaEvent_t ev : walk_ev_) cudaEventDestroy(ev);
   if (ring_h_) cudaFreeHost(ring_h_);
@@ -961,9 +964,30 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   // Segment length: as given, else the shortest (at least 64) that keeps
   // every segment of the call on a resident thread -- one wave per pass.
   int seg_len = o.seg_len;
+  SegTune* tune = nullptr;
+  int tune_slot = -1;
   if (seg_len <= 0) {
     const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0));
-    seg_len = static_cast<int>(std::min<int64_t>(1024, (all_px + resident - 1) / resident));
+    const int rule = static_cast<int>(std::min<int64_t>(16384, (all_px + resident - 1) / resident));
+    int bucket = 0;
+    while ((int64_t{1} << (bucket + 1)) <= all_px) ++bucket;
+    tune = &seg_tune_[std::make_pair(bucket, assoc ? 1 : 0)];
+    if (tune->cand.empty()) {
+      for (int c : {rule, rule / 2, rule / 4, rule * 2}) {
+        c = std::min(16384, (std::max(c, 64) + 15) & ~15);
+        if (std::find(tune->cand.begin(), tune->cand.end(), c) == tune->cand.end()) tune->cand.push_back(c);
+      }
+      tune->ms.assign(tune->cand.size(), -1.0);
+    }
+    for (std::size_t c = 0; c < tune->cand.size() && tune_slot < 0; ++c) {
+      if (tune->ms[c] < 0) tune_slot = static_cast<int>(c);
+    }
+    if (tune_slot >= 0) {
+      seg_len = tune->cand[static_cast<std::size_t>(tune_slot)];
+    } else {
+      seg_len = tune->cand[static_cast<std::size_t>(
+          std::min_element(tune->ms.begin(), tune->ms.end()) - tune->ms.begin())];
+    }
   }
   seg_len = (std::max(seg_len, 64) + 15) & ~15;
   for (int i = 0; i < n; ++i) {
@@ -1120,6 +1144,14 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   };
   int issued = 0, checked = 0;
   bool done = false;
+  // The tuner times the passes on the device (setup and uploads excluded).
+  const bool timing = tune && tune_slot >= 0;
+  if (timing) {
+    for (cudaEvent_t& ev : tune_ev_) {
+      if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return CudaFail(e, "tuner events");
+    }
+    cudaEventRecord(tune_ev_[0], s);
+  }
   while (!done) {
     while (issued < checked + kDepth && issued < max_passes) {
       const int k = issued % kDepth;
@@ -1183,6 +1215,16 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     ++checked;
   }
   const int pass = checked - 1;
+  if (timing) {
+    // The last checked pass's completion event was recorded after its
+    // verification: time from the first pass's start to it.
+    float ms = 0.0f;
+    cudaEventRecord(tune_ev_[1], s);
+    cudaEventSynchronize(tune_ev_[1]);
+    if (cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) == cudaSuccess) {
+      tune->ms[static_cast<std::size_t>(tune_slot)] = ms;
+    }
+  }
   last_passes_ = pass + 1;
   if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
   if (profiling_) {
