@@ -208,14 +208,12 @@ def run_ours(a, rank: int, world: int):
     torch.cuda.synchronize()
     kstats = ctx.stats()
     ctx.profile(False)
-    total_ms = sum(times)
+    from stipple_b200 import replicas
+    total_ms = replicas.max_over_ranks(sum(times))
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
         torch.distributed.barrier()
     px = W * H
-    value = world * px * a.steps / (total_ms / 1e3) / 1e6
+    value = replicas.job_rate(px * a.steps, world, total_ms) / 1e6
     ms_step = total_ms / a.steps
 
     # Reference-facing call with host buffers: H2D + walk + D2H every step.
@@ -228,7 +226,8 @@ def run_ours(a, rank: int, world: int):
         ctx.dither_host_into("seq", pinned_in.numpy(), pid, pinned_out.numpy())
         if k >= w_e2e:
             e2e_t.append(time.perf_counter() - t0)
-    e2e = {"value": world * px * len(e2e_t) / sum(e2e_t) / 1e6, "unit": "Mpixel/s",
+    e2e_ms = replicas.max_over_ranks(sum(e2e_t) * 1e3)
+    e2e = {"value": replicas.job_rate(px * len(e2e_t), world, e2e_ms) / 1e6, "unit": "Mpixel/s",
            "h2d_bytes_per_step": int(img.nbytes), "d2h_bytes_per_step": int(W * H)}
 
     hbm, peak_kind = peaks()
