@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--skip-extra", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="requests in the served-stream sample (the full stream is 10,000)")
-    ap.add_argument("--serve-rates", default="20,60",
+    ap.add_argument("--serve-rates", default="30,120,600",
                     help="Poisson arrival rates (requests/s) of the served-stream sample")
     ap.add_argument("--profile-case", default="none", choices=["none", "seq", "seq_alpha", "blocks", "batched"],
                     help="run only that workload's device steps (for ncu captures) and print "

@@ -2,6 +2,9 @@
 #include "rdb_runtime.h"
 
 #include <algorithm>
+#include <map>
+#include <tuple>
+#include <mutex>
 #include <cstring>
 #include <numeric>
 
@@ -23,6 +26,16 @@ std::size_t RowStride(const rdb_job& j) {
 }
 
 }  // namespace
+
+std::mutex& SegTuneLock() {
+  static std::mutex mu;
+  return mu;
+}
+
+std::map<std::tuple<int, int, int>, SegTune>& SegTuneTable() {
+  static std::map<std::tuple<int, int, int>, SegTune> table;
+  return table;
+}
 
 std::size_t BytesPerPixel(int layout) { return layout == RDB_RGBAF32 ? 16 : static_cast<std::size_t>(layout); }
 
@@ -971,7 +984,8 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     const int rule = static_cast<int>(std::min<int64_t>(16384, (all_px + resident - 1) / resident));
     int bucket = 0;
     while ((int64_t{1} << (bucket + 1)) <= all_px) ++bucket;
-    tune = &seg_tune_[std::make_pair(bucket, assoc ? 1 : 0)];
+    std::lock_guard<std::mutex> lk(SegTuneLock());
+    tune = &SegTuneTable()[std::make_tuple(device_, bucket, assoc ? 1 : 0)];
     if (tune->cand.empty()) {
       for (int c : {rule, rule / 2, rule / 4, rule * 2}) {
         c = std::min(16384, (std::max(c, 64) + 15) & ~15);
@@ -980,13 +994,21 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       tune->ms.assign(tune->cand.size(), -1.0);
     }
     for (std::size_t c = 0; c < tune->cand.size() && tune_slot < 0; ++c) {
-      if (tune->ms[c] < 0) tune_slot = static_cast<int>(c);
+      if (tune->ms[c] == -1.0) tune_slot = static_cast<int>(c);
     }
     if (tune_slot >= 0) {
+      tune->ms[static_cast<std::size_t>(tune_slot)] = -2.0;
       seg_len = tune->cand[static_cast<std::size_t>(tune_slot)];
     } else {
-      seg_len = tune->cand[static_cast<std::size_t>(
-          std::min_element(tune->ms.begin(), tune->ms.end()) - tune->ms.begin())];
+      // Fastest measured (others may still be under measurement).
+      int best = 0;
+      for (std::size_t c = 0; c < tune->cand.size(); ++c) {
+        if (tune->ms[c] >= 0 && (tune->ms[static_cast<std::size_t>(best)] < 0 ||
+                                 tune->ms[c] < tune->ms[static_cast<std::size_t>(best)])) {
+          best = static_cast<int>(c);
+        }
+      }
+      seg_len = tune->cand[static_cast<std::size_t>(best)];
     }
   }
   seg_len = (std::max(seg_len, 64) + 15) & ~15;
@@ -1221,9 +1243,9 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     float ms = 0.0f;
     cudaEventRecord(tune_ev_[1], s);
     cudaEventSynchronize(tune_ev_[1]);
-    if (cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) == cudaSuccess) {
-      tune->ms[static_cast<std::size_t>(tune_slot)] = ms;
-    }
+    std::lock_guard<std::mutex> lk(SegTuneLock());
+    tune->ms[static_cast<std::size_t>(tune_slot)] =
+        cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) == cudaSuccess ? ms : -1.0;
   }
   last_passes_ = pass + 1;
   if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");

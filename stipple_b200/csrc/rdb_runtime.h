@@ -41,6 +41,17 @@ struct DevPlan {
   uint8_t* uniform = nullptr;  // uniform-key table (rdb_uniform.h), built on first use
 };
 
+// Segment-length autotuner of the segmented walk: per (device, log2 of the
+// call's pixels, alpha) it times the occupancy rule's length, a half, a
+// quarter and twice that on the first calls (device time of the passes) and
+// keeps the fastest.  Results are exact whichever length runs, so exploring
+// costs time only.  The table is shared by every context of the process
+// (one lock), so the device workers of a server do not each explore afresh.
+struct SegTune {
+  std::vector<int> cand;
+  std::vector<double> ms;  // -1 = not yet measured, -2 = being measured
+};
+
 class Context {
  public:
   ~Context();
@@ -140,16 +151,6 @@ class Context {
   cudaEvent_t ev_[2] = {nullptr, nullptr};
   // Pipelined pass loop of the segmented walk: a pinned ring of per-pass
   // results and the events that mark each pass done (and time its walk).
-  // Segment-length autotuner of the segmented walk: per (log2 of the call's
-  // pixels, alpha) it times the occupancy rule's length, a half, a quarter and
-  // twice that on the first calls (device time of the passes) and keeps the
-  // fastest.  Results are exact whichever
-  // length runs, so exploring costs time only.
-  struct SegTune {
-    std::vector<int> cand;
-    std::vector<double> ms;  // < 0 = not yet measured
-  };
-  std::map<std::pair<int, int>, SegTune> seg_tune_;
   cudaEvent_t tune_ev_[2] = {nullptr, nullptr};
   int PinnedRing(std::size_t ints);
   int PassEvents(int depth);
