@@ -194,7 +194,6 @@ def run_ours(a, rank: int, world: int):
     if world > 1:
         torch.distributed.barrier()
     times = []
-    ctx.profile(True)  # walk-kernel events on the launching stream, launch counts
     with ClockSampler(dev) as clk:
         for _ in range(a.steps):
             flush.fill_(1)
@@ -206,6 +205,15 @@ def run_ours(a, rank: int, world: int):
             ctx.synchronize(s)
             times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
+    # Kernel-level figures: the same step once more with the context's
+    # profiling on -- the host then checks each pass and records CUDA events
+    # around every walk launch on its stream (the timed steps above run the
+    # device-side pass loop, one graph launch, where no event can sit between
+    # two of its kernels).  Same kernels, same launches, same passes.
+    ctx.profile(True)
+    flush.fill_(1)
+    step_dev()
+    ctx.synchronize(s)
     kstats = ctx.stats()
     ctx.profile(False)
     from stipple_b200 import replicas
@@ -246,13 +254,15 @@ def run_ours(a, rank: int, world: int):
                 "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "TswWalkKernel", "walk_ms_per_launch": walk_ms,
                 "positions_per_launch": pos_per_launch,
+                "measured_on": "one extra step after the timed ones, host-checked pass loop, "
+                               "CUDA events around each walk launch on its stream",
                 "note": "each segment is a dependent chain walked by one thread: the kernel "
                         "is bound by the per-step chain latency, not HBM (see chain); DRAM "
                         "traffic per launch is in profiles/"}
     clock = clk.summary()["sm_mhz"]
     seg = int(kstats["seg_len"])
-    chain = {"passes_per_step": kstats["passes"] / max(1, a.steps), "ns_per_px": ms_step * 1e6 / px,
-             "walk_share": kstats["walk_ms"] / total_ms if total_ms else None,
+    chain = {"passes_per_step": kstats["passes"], "ns_per_px": ms_step * 1e6 / px,
+             "walk_share": kstats["walk_ms"] / (total_ms / a.steps) if total_ms else None,
              "segment_len": seg, "concurrent_chains": int(kstats["chains"]), "clock_mhz": clock}
     if clock and walk_ms > 0 and seg:
         # A launch walks every unverified segment once: seg steps per chain.
@@ -269,7 +279,7 @@ def run_ours(a, rank: int, world: int):
                       "warmup_steps_run": max(5, a.warmup),
                       "parallelism": f"replicas x{world}"},
            "e2e": e2e, "roofline": roofline, "chain": chain, "clocks": clk.summary(),
-           "gpu_launches": int(kstats["launches"])}
+           "gpu_launches": int(kstats["launches"]) * a.steps}
 
     if rank == 0 and not a.skip_extra:
         out["blocks"] = bench_blocks(ctx, s, a, tree, pid, hbm)

@@ -6,7 +6,8 @@
  * or an RDB_E_* code; rdb_last_error() then gives a human-readable message
  * for the calling thread.  The reference's engine API (include/rd_riemersma.h
  * of rdither) reports errors as a std::string that is empty on success; the
- * C++ drop-in layer (rd_dropin.cpp) maps these codes back to that form.
+ * C++ drop-in layer (stipple_b200/dropin/rd_b200_dropin.cpp) maps these codes
+ * back to that form.
  *
  * Each declaration names the reference interface it stands in for.
  */
@@ -176,7 +177,13 @@ typedef struct rdb_options {
   int warm_len;         /* segmented walk: warm-up positions before each segment, 0 = auto */
   int max_passes;       /* segmented walk: give up after this many passes (0 = no limit); the
                            walk then reports RDB_E_DEVICE -- never an inexact result */
-  int reserved[4];
+  int loop_mode;        /* segmented thread walk: 0 = automatic (the device-side loop below
+                           unless the context is profiling), 1 = the host checks each pass,
+                           2 = the device-side loop: one CUDA graph whose while-conditional
+                           node repeats the passes until a control kernel sees convergence,
+                           so the call returns without waiting for the device (errors then
+                           surface at rdb_synchronize) */
+  int reserved[3];
 } rdb_options;
 
 void rdb_options_default(rdb_options* o);

@@ -51,7 +51,8 @@ class Options(C.Structure):
         ("seg_len", C.c_int),
         ("warm_len", C.c_int),
         ("max_passes", C.c_int),
-        ("reserved", C.c_int * 4),
+        ("loop_mode", C.c_int),
+        ("reserved", C.c_int * 3),
     ]
 
 

@@ -180,7 +180,9 @@ void rdb_context_destroy(rdb_context* ctx) { delete ctx; }
 
 size_t rdb_context_bytes(const rdb_context* ctx) { return ctx ? ctx->impl.bytes() : 0; }
 
-int rdb_context_last_passes(const rdb_context* ctx) { return ctx ? ctx->impl.last_passes() : 0; }
+int rdb_context_last_passes(const rdb_context* ctx) {
+  return ctx ? const_cast<rdb_context*>(ctx)->impl.last_passes() : 0;
+}
 
 int rdb_context_profile(rdb_context* ctx, int enable) {
   if (!ctx) return Guard("rdb_context_profile");
@@ -294,6 +296,7 @@ void rdb_options_default(rdb_options* o) {
   o->seg_len = 0;
   o->warm_len = 0;
   o->max_passes = 0;
+  o->loop_mode = 0;
 }
 
 int rdb_dither(rdb_context* ctx, int engine, const rdb_job* jobs, int n_jobs,

@@ -76,6 +76,8 @@ Context::~Context() {
   for (cudaEvent_t& ev : ev_) {
     if (ev) cudaEventDestroy(ev);
   }
+  if (loop_exec_) cudaGraphExecDestroy(loop_exec_);
+  Release(&tsw_ctl_);
   for (cudaEvent_t ev : pass_ev_) cudaEventDestroy(ev);
   for (cudaEvent_t ev : tune_ev_) {
     if (ev) cudaEventDestroy(ev);
@@ -84,6 +86,19 @@ Context::~Context() {
   for (cudaEvent_t ev : walk_ev_) cudaEventDestroy(ev);
   if (ring_h_) cudaFreeHost(ring_h_);
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Context::last_passes() {
+  if (loop_pending_) {
+    int words[3] = {0, 0, 0};
+    cudaSetDevice(device_);
+    if (cudaStreamSynchronize(loop_stream_) == cudaSuccess &&
+        cudaMemcpy(words, tsw_ctl_.ptr, sizeof(words), cudaMemcpyDeviceToHost) == cudaSuccess) {
+      last_passes_ = 2 + words[2];  // two passes enqueued by the host, then the loop's
+    }
+    loop_pending_ = false;
+  }
+  return last_passes_;
 }
 
 int Context::PinnedRing(std::size_t ints) {
@@ -1147,6 +1162,78 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   }
   if ((e = LaunchTswGather(L, positions, s)) != cudaSuccess) return CudaFail(e, "sample gather");
 
+  // The tuner times the passes on the device (setup and uploads excluded).
+  const bool timing = tune && tune_slot >= 0;
+  if (timing) {
+    for (cudaEvent_t& ev : tune_ev_) {
+      if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return CudaFail(e, "tuner events");
+    }
+    cudaEventRecord(tune_ev_[0], s);
+  }
+  const int max_passes_opt = o.max_passes > 0 ? o.max_passes : 1 << 30;
+  const bool device_loop = o.loop_mode == 2 || (o.loop_mode == 0 && !profiling_);
+  if (o.loop_mode < 0 || o.loop_mode > 2) return Fail(RDB_E_INVALID, "loop_mode must be 0..2");
+  if (device_loop) {
+    // Passes 0 and 1 from the host (pass 0 is the warm-up pass), then the
+    // rest as one graph launch: nothing here waits for the device.
+    for (int pass = 0; pass < 2; ++pass) {
+      L.pass = pass;
+      L.tag = static_cast<uint32_t>(pass + 1);
+      cudaMemsetAsync(L.bad[pass & 1], 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
+      if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
+      if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
+      if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
+    }
+    if (int rc = Reserve(&tsw_ctl_, 64, "loop control")) return rc;
+    static const int kCtlInit[8] = {0, 0, 0, 0, 3, 0, 0, 0};  // counters, then the tag of pass 2
+    int* ctl = static_cast<int*>(tsw_ctl_.ptr);
+    uint32_t* tag_dev = reinterpret_cast<uint32_t*>(ctl + 4);
+    if ((e = cudaMemcpyAsync(ctl, kCtlInit, sizeof(kCtlInit), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+      return CudaFail(e, "loop control");
+    }
+    TswLaunch even = L, odd = L;
+    even.pass = 2;
+    odd.pass = 3;
+    even.tag_dev = odd.tag_dev = tag_dev;
+    const int loop_max = std::max(1, max_passes_opt - 2);
+    // The executable graph is rebuilt only when the launch parameters change.
+    std::vector<unsigned char> key(sizeof(TswLaunch) + 2 * sizeof(int));
+    std::memcpy(key.data(), &even, sizeof(TswLaunch));
+    std::memcpy(key.data() + sizeof(TswLaunch), &total, sizeof(int));
+    std::memcpy(key.data() + sizeof(TswLaunch) + sizeof(int), &loop_max, sizeof(int));
+    if (!loop_exec_ || key != loop_key_) {
+      if (loop_exec_) {
+        cudaGraphExecDestroy(loop_exec_);
+        loop_exec_ = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      if ((e = BuildTswLoopGraph(even, odd, total, ctl, tag_dev, loop_max, &g)) != cudaSuccess) {
+        return CudaFail(e, "pass-loop graph");
+      }
+      e = cudaGraphInstantiate(&loop_exec_, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        loop_exec_ = nullptr;
+        return CudaFail(e, "pass-loop graph instantiation");
+      }
+      loop_key_ = key;
+    }
+    if ((e = cudaGraphLaunch(loop_exec_, s)) != cudaSuccess) return CudaFail(e, "pass-loop graph launch");
+    if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
+    loop_pending_ = true;
+    loop_stream_ = s;
+    if (timing) {
+      // The tuner still needs this length's time: wait for it here.
+      cudaEventRecord(tune_ev_[1], s);
+      cudaEventSynchronize(tune_ev_[1]);
+      float ms = 0.0f;
+      std::lock_guard<std::mutex> lk(SegTuneLock());
+      tune->ms[static_cast<std::size_t>(tune_slot)] =
+          cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) == cudaSuccess ? ms : -1.0;
+    }
+    return RDB_OK;
+  }
+
   // Passes are enqueued up to kDepth ahead of the one the host is checking:
   // every kernel takes its verified prefix from the device's own result of
   // the previous pass, so the host only has to learn when to stop.  Each pass
@@ -1166,14 +1253,6 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   };
   int issued = 0, checked = 0;
   bool done = false;
-  // The tuner times the passes on the device (setup and uploads excluded).
-  const bool timing = tune && tune_slot >= 0;
-  if (timing) {
-    for (cudaEvent_t& ev : tune_ev_) {
-      if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return CudaFail(e, "tuner events");
-    }
-    cudaEventRecord(tune_ev_[0], s);
-  }
   while (!done) {
     while (issued < checked + kDepth && issued < max_passes) {
       const int k = issued % kDepth;

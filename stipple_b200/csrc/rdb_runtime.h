@@ -152,6 +152,13 @@ class Context {
   // Pipelined pass loop of the segmented walk: a pinned ring of per-pass
   // results and the events that mark each pass done (and time its walk).
   cudaEvent_t tune_ev_[2] = {nullptr, nullptr};
+  // Device-side pass loop: control words, the cached executable graph and the
+  // launch parameters it was built for.
+  DevBuf tsw_ctl_;
+  cudaGraphExec_t loop_exec_ = nullptr;
+  std::vector<unsigned char> loop_key_;
+  bool loop_pending_ = false;       // last_passes_ still to be read from the device
+  cudaStream_t loop_stream_ = nullptr;
   int PinnedRing(std::size_t ints);
   int PassEvents(int depth);
   int* ring_h_ = nullptr;
@@ -162,7 +169,9 @@ class Context {
   std::vector<cudaEvent_t> walk_ev_;
 
  public:
-  int last_passes() const { return last_passes_; }
+  // Passes of the last segmented walk; after a device-side loop this waits
+  // for that call's stream and reads the loop's own count.
+  int last_passes();
   int Profile(bool on);
   const rdb_kernel_stats& stats() const { return stats_; }
 };

@@ -228,7 +228,7 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   uint64_t* ot = L.own + (static_cast<int64_t>(sid) << L.own_bits);
   uint32_t* ol = L.own_list + (static_cast<int64_t>(sid) << L.own_bits);
   const unsigned omask = (1u << L.own_bits) - 1u;
-  const uint64_t tag = static_cast<uint64_t>(L.tag) << 32;
+  const uint64_t tag = static_cast<uint64_t>(L.tag_dev ? *L.tag_dev : L.tag) << 32;
   double* qe = L.q_end[L.pass & 1] + static_cast<int64_t>(sid) * 64;
   double* qs = L.q_start + static_cast<int64_t>(sid) * 64;
   uint8_t* out = L.chosen + base;
@@ -538,6 +538,48 @@ __global__ void TswScatter(TswLaunch L, int64_t total) {
   }
 }
 
+// The loop's control step (see BuildTswLoopGraph), one block.
+__global__ void TswControl(TswLaunch L, cudaGraphConditionalHandle handle, int* ctl,
+                           uint32_t* tag_dev, int max_passes) {
+  __shared__ int done_all, stalled_any;
+  if (threadIdx.x == 0) {
+    done_all = 1;
+    stalled_any = 0;
+  }
+  __syncthreads();
+  const bool finished = ctl[1] != 0;
+  if (!finished) {
+    const int* cur = L.bad[L.pass & 1];
+    const int* prev = L.bad[(L.pass & 1) ^ 1];
+    for (int i = threadIdx.x; i < L.n_images; i += blockDim.x) {
+      const int ns = L.images[i].nsegs;
+      const int nf = min(cur[i], ns);
+      const int of = min(prev[i], ns);
+      if (nf < ns) {
+        atomicAnd(&done_all, 0);
+        if (nf <= of) atomicOr(&stalled_any, 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  if (finished) {
+    cudaGraphSetConditional(handle, 0);
+    return;
+  }
+  const int passes = ++ctl[0];
+  if (done_all) {
+    ctl[1] = 1;
+    ctl[2] = passes;
+    cudaGraphSetConditional(handle, 0);
+  } else if (stalled_any || passes >= max_passes) {
+    ctl[1] = 1;
+    atomicExch(L.status, stalled_any ? kDevBadItem : kDevTimeout);
+    cudaGraphSetConditional(handle, 0);
+  }
+  *tag_dev += 1u;
+}
+
 template <bool kFloat, bool kAssoc>
 cudaError_t LaunchWalk(const TswLaunch& L, int smem, cudaStream_t s) {
   const cudaError_t e = AllowMaxSmem(TswWalkKernel<kFloat, kAssoc>);
@@ -593,6 +635,111 @@ cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) 
   if (total_segs <= 0) return cudaSuccess;
   TswVerifySegments<<<(total_segs + 7) / 8, 256, 0, s>>>(L, total_segs);
   return cudaGetLastError();
+}
+
+namespace {
+
+cudaError_t AddKernel(cudaGraph_t g, cudaGraphNode_t* last, const void* func, dim3 grid,
+                      dim3 block, unsigned smem, void** args) {
+  cudaKernelNodeParams kp{};
+  kp.func = const_cast<void*>(func);
+  kp.gridDim = grid;
+  kp.blockDim = block;
+  kp.sharedMemBytes = smem;
+  kp.kernelParams = args;
+  cudaGraphNode_t node;
+  const cudaError_t e = cudaGraphAddKernelNode(&node, g, *last ? last : nullptr, *last ? 1 : 0, &kp);
+  if (e == cudaSuccess) *last = node;
+  return e;
+}
+
+template <bool kFloat, bool kAssoc>
+const void* WalkFunc() {
+  return reinterpret_cast<const void*>(TswWalkKernel<kFloat, kAssoc>);
+}
+
+// One pass into graph g after *last: clear this parity's failures, prepare,
+// walk, check, control.
+cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int total_segs,
+                    cudaGraphConditionalHandle* h, int** ctl, uint32_t** tag_dev, int* max_passes) {
+  cudaMemsetParams ms{};
+  ms.dst = L->bad[L->pass & 1];
+  ms.value = 0x7F;
+  ms.elementSize = 1;
+  ms.width = static_cast<std::size_t>(L->n_images) * sizeof(int);
+  ms.height = 1;
+  cudaGraphNode_t node;
+  cudaError_t e = cudaGraphAddMemsetNode(&node, g, *last ? last : nullptr, *last ? 1 : 0, &ms);
+  if (e != cudaSuccess) return e;
+  *last = node;
+  void* args1[] = {L};
+  if (L->use_cache && L->n_images > 0) {
+    e = AddKernel(g, last, reinterpret_cast<const void*>(TswPrepare), dim3(kKeys / 256, L->n_images),
+                  dim3(256), 0, args1);
+    if (e != cudaSuccess) return e;
+  }
+  if (L->n_chunks > 0) {
+    const void* wf = L->assoc ? (L->is_float ? WalkFunc<true, true>() : WalkFunc<false, true>())
+                              : (L->is_float ? WalkFunc<true, false>() : WalkFunc<false, false>());
+    e = AddKernel(g, last, wf, dim3(L->n_chunks), dim3(L->chunk_threads),
+                  static_cast<unsigned>(TswSmemBytes(L->plan_smem_max)), args1);
+    if (e != cudaSuccess) return e;
+  }
+  if (L->use_cache && L->n_images > 0) {
+    e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifyKeys), dim3(kKeys / 256, L->n_images),
+                  dim3(256), 0, args1);
+    if (e != cudaSuccess) return e;
+  }
+  if (total_segs > 0) {
+    void* args2[] = {L, &total_segs};
+    e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifySegments), dim3((total_segs + 7) / 8),
+                  dim3(256), 0, args2);
+    if (e != cudaSuccess) return e;
+  }
+  void* args3[] = {L, h, ctl, tag_dev, max_passes};
+  return AddKernel(g, last, reinterpret_cast<const void*>(TswControl), dim3(1), dim3(256), 0, args3);
+}
+
+}  // namespace
+
+cudaError_t BuildTswLoopGraph(const TswLaunch& even, const TswLaunch& odd, int total_segs,
+                              int* ctl, uint32_t* tag_dev, int max_passes, cudaGraph_t* out) {
+  cudaError_t e;
+  if (even.n_chunks > 0) {
+    if ((e = even.assoc ? (even.is_float ? AllowMaxSmem(TswWalkKernel<true, true>)
+                                         : AllowMaxSmem(TswWalkKernel<false, true>))
+                        : (even.is_float ? AllowMaxSmem(TswWalkKernel<true, false>)
+                                         : AllowMaxSmem(TswWalkKernel<false, false>))) != cudaSuccess) {
+      return e;
+    }
+  }
+  cudaGraph_t g = nullptr;
+  if ((e = cudaGraphCreate(&g, 0)) != cudaSuccess) return e;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return e;
+  }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  if ((e = cudaGraphAddNode(&cnode, g, nullptr, 0, &cp)) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return e;
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  TswLaunch L0 = even, L1 = odd;
+  cudaGraphNode_t last = nullptr;
+  if ((e = AddPass(body, &last, &L0, total_segs, &h, &ctl, &tag_dev, &max_passes)) != cudaSuccess ||
+      (e = AddPass(body, &last, &L1, total_segs, &h, &ctl, &tag_dev, &max_passes)) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return e;
+  }
+  *out = g;
+  return cudaSuccess;
 }
 
 cudaError_t LaunchTswScatter(const TswLaunch& L, int64_t total, cudaStream_t s) {

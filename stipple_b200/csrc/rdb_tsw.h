@@ -100,6 +100,8 @@ struct TswLaunch {
   // prefix -- and writes bad[p & 1].
   int* bad[2];
   int* status;
+  // Device-side loop: the own-table tag of the running pass (null: use `tag`).
+  const uint32_t* tag_dev;
   double sw[16];
 };
 
@@ -115,5 +117,19 @@ cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s);
 cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s);
 // Indices (and RgbaF output) of every position into the images.
 cudaError_t LaunchTswScatter(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
+
+// The pass loop as one CUDA graph: a while-conditional node whose body runs
+// an even-parity pass, a control kernel, an odd-parity pass and the control
+// kernel again.  `even` and `odd` are the launch parameters of the two
+// passes (`pass` of matching parity and not 0; `tag_dev` set).  The control
+// kernel (one block) reads every image's first failure of the pass just
+// run: all images verified -> it stops the loop and records the pass count;
+// an unfinished image whose verified prefix did not grow, or `max_passes`
+// passes run -> it sets the status word and stops the loop; otherwise it
+// advances the tag.  ctl[0] counts the loop's passes, ctl[1] is set once the
+// loop is finished (later control launches then only stop it), ctl[2] is the
+// loop's pass count at convergence.
+cudaError_t BuildTswLoopGraph(const TswLaunch& even, const TswLaunch& odd, int total_segs,
+                              int* ctl, uint32_t* tag_dev, int max_passes, cudaGraph_t* out);
 
 }  // namespace rdb

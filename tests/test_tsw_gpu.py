@@ -168,3 +168,26 @@ def test_thread_segmented_mixed_alpha_batch(ctx, oracle):
     finally:
         for p in pids:
             ctx.release_palette(p)
+
+
+@pytest.mark.parametrize("alpha", [False, True])
+def test_host_and_device_pass_loops_agree(ctx, oracle, alpha):
+    """The pass loop checked by the host (loop_mode=1) and the device-side loop
+    in one CUDA graph (loop_mode=2) give the oracle's bytes; the device loop's
+    pass limit surfaces as an error, never as an inexact result."""
+    img = synth.gradient_rgba8(480, 320, 9) if alpha else synth.gradient_rgb8(480, 320, 9)
+    t = sb.Octree(img, 64, alpha)
+    pid = ctx.palette_from_octree(t)
+    try:
+        want, _, _ = oracle.walk_seq(synth.to_q16(img), 64, alpha, t.grayscale)
+        for mode in (1, 2, 2):  # the second device-loop call reuses the cached graph
+            got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=64, warm_len=16, loop_mode=mode)
+            assert np.array_equal(got, want), mode
+            assert ctx.last_passes >= 3
+        with pytest.raises(sb.RdbError):
+            ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=64, warm_len=16, loop_mode=2,
+                            max_passes=3)
+        got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=64, warm_len=16, loop_mode=2)
+        assert np.array_equal(got, want)  # the context recovers after the error
+    finally:
+        ctx.release_palette(pid)
