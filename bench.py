@@ -50,9 +50,11 @@ def parse():
                     help="requests in the served-stream sample (the full stream is 10,000)")
     ap.add_argument("--serve-rates", default="30,120,600",
                     help="Poisson arrival rates (requests/s) of the served-stream sample")
-    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "seq_alpha", "blocks", "batched"],
+    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "seq_alpha", "blocks", "batched", "jacobi"],
                     help="run only that workload's device steps (for ncu captures) and print "
                          "its timing; no JSON contract line")
+    ap.add_argument("--seq-mode", type=int, default=0, help="profile cases: sequential form")
+    ap.add_argument("--size", default="3840x2160", help="profile cases: frame size WxH")
     return ap.parse_args()
 
 
@@ -467,7 +469,8 @@ def profile_case(a):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     s = stream.cuda_stream
-    W, H, C = HEADLINE["width"], HEADLINE["height"], HEADLINE["colors"]
+    W, H = (int(v) for v in a.size.lower().split("x"))
+    C = HEADLINE["colors"]
     img = synth.gradient_rgb8(W, H, HEADLINE["seed"])
     pid = ctx.palette_from_octree(sb.Octree(img, C, False, False))
     if a.profile_case == "batched":
@@ -483,7 +486,7 @@ def profile_case(a):
             jobs.append(dict(pixels=d.data_ptr(), width=w, height=h, layout=sb.RGBA8, palette_id=p,
                              indices=o.data_ptr()))
         opts = {}
-    elif a.profile_case in ("seq", "seq_alpha"):
+    elif a.profile_case in ("seq", "seq_alpha", "jacobi"):
         lay = sb.RGB8
         if a.profile_case == "seq_alpha":
             img = synth.gradient_rgba8(W, H, HEADLINE["seed"])
@@ -493,7 +496,7 @@ def profile_case(a):
         o = torch.empty((H, W), dtype=torch.uint8, device="cuda")
         jobs = [dict(pixels=d.data_ptr(), width=W, height=H, layout=lay, palette_id=pid,
                      indices=o.data_ptr())]
-        opts = {}
+        opts = {"seq_mode": a.seq_mode} if a.profile_case != "jacobi" else {}
     else:
         n = a.block_frames
         frames = [torch.from_numpy(synth.video_frame(W, H, 3, f)).cuda() for f in range(n)]
@@ -501,7 +504,7 @@ def profile_case(a):
         jobs = [dict(pixels=f.data_ptr(), width=W, height=H, layout=sb.RGB8, palette_id=pid,
                      indices=x.data_ptr()) for f, x in zip(frames, outs)]
         opts = {"block": 256}
-    engine = "blocks" if a.profile_case == "blocks" else "seq"
+    engine = {"blocks": "blocks", "jacobi": "jacobi"}.get(a.profile_case, "seq")
     for _ in range(a.warmup):
         ctx.dither(engine, jobs, stream=s, **opts)
     ctx.synchronize(s)
