@@ -55,6 +55,9 @@ def parse():
                          "its timing; no JSON contract line")
     ap.add_argument("--seq-mode", type=int, default=0, help="profile cases: sequential form")
     ap.add_argument("--size", default="3840x2160", help="profile cases: frame size WxH")
+    ap.add_argument("--loop-mode", type=int, default=0,
+                    help="profile cases: segmented walk pass loop (1 = host-checked, so ncu "
+                         "sees every pass as its own launch; 2 = device-side graph)")
     return ap.parse_args()
 
 
@@ -496,7 +499,7 @@ def profile_case(a):
         o = torch.empty((H, W), dtype=torch.uint8, device="cuda")
         jobs = [dict(pixels=d.data_ptr(), width=W, height=H, layout=lay, palette_id=pid,
                      indices=o.data_ptr())]
-        opts = {"seq_mode": a.seq_mode} if a.profile_case != "jacobi" else {}
+        opts = {"seq_mode": a.seq_mode, "loop_mode": a.loop_mode} if a.profile_case != "jacobi" else {}
     else:
         n = a.block_frames
         frames = [torch.from_numpy(synth.video_frame(W, H, 3, f)).cuda() for f in range(n)]
