@@ -322,6 +322,62 @@ def bench_blocks(ctx, s, a, tree, pid, hbm):
         gbs = px * 4 / (ms / 1e3) / 1e9
         res[f"B{B}"] = {"ms": ms, "mpx_s": px / ms / 1e3, "gb_s": gbs, "hbm_frac": gbs / hbm}
     res["workload"] = f"{n} frames of 3840x2160 RGB8 video, fixed 256-colour palette"
+    res["video_formats"] = bench_frames(ctx, s, a, pid)
+    return res
+
+
+def bench_frames(ctx, s, a, pid):
+    """The block engine on the decoder's / encoder's own formats (planar
+    4:4:4 in, planar 4:4:4 out: 3 B/px each way) against the RgbaF form the
+    reference's callers otherwise convert through (16 B/px each way), B = 512,
+    device-timed and end to end through the host-buffer call from pinned
+    memory."""
+    import torch
+    import stipple_b200 as sb
+    from stipple_b200 import synth
+    W, H = HEADLINE["width"], HEADLINE["height"]
+    n = a.block_frames
+    yuv = np.stack([synth.yuv444_frame(synth.video_frame(W, H, 3, f)).reshape(-1)
+                    for f in range(n)])
+    fb = sb.frame_bytes(sb.YUV444P8, W, H)
+    d_in = torch.from_numpy(yuv).cuda()
+    d_out = torch.empty((n, fb), dtype=torch.uint8, device="cuda")
+    res = {"workload": f"{n} frames of 3840x2160, planar YCbCr 4:4:4 in and out, B=512"}
+    for _ in range(2):
+        ctx.dither_frames(d_in.data_ptr(), sb.YUV444P8, W, H, n, pid, d_out.data_ptr(),
+                          sb.YUV444P8, stream=s, block=512)
+    ctx.synchronize(s)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.current_stream())
+    ctx.dither_frames(d_in.data_ptr(), sb.YUV444P8, W, H, n, pid, d_out.data_ptr(),
+                      sb.YUV444P8, stream=s, block=512)
+    e1.record(torch.cuda.current_stream())
+    ctx.synchronize(s)
+    ms = e0.elapsed_time(e1)
+    res["device_mpx_s"] = n * W * H / ms / 1e3
+    del d_in, d_out
+
+    def e2e(inp, in_fmt, out_fmt):
+        out = torch.empty((n, sb.frame_bytes(out_fmt, W, H)), dtype=torch.uint8).pin_memory()
+        ctx.dither_frames_host(inp.numpy(), in_fmt, W, H, pid, out_fmt, out=out.numpy(), block=512)
+        t = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            ctx.dither_frames_host(inp.numpy(), in_fmt, W, H, pid, out_fmt, out=out.numpy(),
+                                   block=512)
+            t.append(time.perf_counter() - t0)
+        return {"mpx_s": n * W * H / min(t) / 1e6, "h2d_bytes": int(inp.numel()),
+                "d2h_bytes": int(out.numel())}
+
+    pin_yuv = torch.from_numpy(yuv).pin_memory()
+    res["e2e_yuv444"] = e2e(pin_yuv, sb.YUV444P8, sb.YUV444P8)
+    del pin_yuv
+    rgbaf = torch.empty((n, W * H * 16), dtype=torch.uint8).pin_memory()
+    for f in range(n):
+        rgbaf[f].numpy().view(np.float32)[:] = synth.to_q16(
+            synth.video_frame(W, H, 3, f)).reshape(-1)
+    res["e2e_rgbaf"] = e2e(rgbaf, sb.RGBAF32, sb.RGBAF32)
     return res
 
 

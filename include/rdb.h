@@ -220,6 +220,56 @@ typedef struct rdb_host_job {
 int rdb_dither_host(rdb_context* ctx, int engine, const rdb_host_job* jobs, int n_jobs,
                     const rdb_options* opts);
 
+/* ---- video frames through the blocks engine ------------------------------
+ * A batch of equal-size frames in the decoder's own format, dithered by the
+ * blocks engine and written in the encoder's own format: the input is widened
+ * to Q16 floats per visit and the output narrowed per pixel inside the
+ * engine's gather and scatter, so no RgbaF frame exists on either side.
+ * Replaces RiemersmaBlocksCuda's upload_u16 / in_mode / emit_u16 /
+ * emit_yuv444 forms (include/rd_riemersma.h:325-464) and RiemersmaBlocksCpu's
+ * gather_raw / raw_out arguments (:224-268), byte for byte with the latter:
+ *   in   RGB16 / RGBA16   each uint16 widened as a float; alpha 65535 if absent
+ *        YUV444P8         swscale's 8-bit YCbCr -> 16-bit RGB (rd_types.h:75-97)
+ *        YUV420P8         chroma upsampled 2x bilinearly first
+ *                         (src/rd_blocks_cuda.cu:660-706); even sizes only
+ *        RGB8 / RGBA8 / RGBAF32 as for rdb_dither
+ *   out  RGBA16           uint16 of the colour's Q16 float; alpha from the
+ *                         palette when it associates alpha, else the source's
+ *        YUV444P8         BT.601 limited range of the colour's top 8 bits
+ *        RGBAF32          the rdb_dither result (may equal `in` for RGBAF32 in)
+ * The cell the block list never visits takes its source value in the output
+ * format (src/rd_riemersma_cpu.cpp:755-801).  Frames are packed: planar
+ * formats hold Y, Cb, Cr planes of width*height bytes (4:4:4) or width*height
+ * and two of width*height/4 (4:2:0) per frame. */
+#define RDB_RGB16 6      /* rgb48le, 3 uint16 per pixel (frames only) */
+#define RDB_RGBA16 8     /* rgba64le, 4 uint16 per pixel (frames only) */
+#define RDB_YUV444P8 444 /* planar 8-bit YCbCr 4:4:4 (frames only) */
+#define RDB_YUV420P8 420 /* planar 8-bit YCbCr 4:2:0, input only (frames only) */
+
+typedef struct rdb_frames {
+  const void* in;          /* `frames` frames, in_frame_bytes apart */
+  size_t in_frame_bytes;   /* 0 = packed (rdb_frame_bytes) */
+  int in_format;
+  int width;
+  int height;
+  int frames;
+  int palette_id;          /* at most 256 colours (one index byte per pixel) */
+  int out_format;          /* RDB_RGBA16, RDB_YUV444P8 or RDB_RGBAF32 */
+  void* out;               /* `frames` frames, out_frame_bytes apart */
+  size_t out_frame_bytes;  /* 0 = packed */
+  uint8_t* indices;        /* optional index map, width*height per frame */
+} rdb_frames;
+
+/* Bytes of one packed frame of `format`, or 0 for an unknown format. */
+size_t rdb_frame_bytes(int format, int width, int height);
+
+/* Device buffers; asynchronous on `stream` like rdb_dither. */
+int rdb_dither_frames(rdb_context* ctx, const rdb_frames* f, const rdb_options* opts,
+                      void* stream);
+/* Host buffers: uploads `in`, dithers, downloads `out` (and `indices`).
+ * Synchronous. */
+int rdb_dither_frames_host(rdb_context* ctx, const rdb_frames* f, const rdb_options* opts);
+
 /* ---- serving ----------------------------------------------------------------
  * A request loop over one device: requests of mixed sizes, palettes and
  * engines are submitted from any thread; host threads build each request's

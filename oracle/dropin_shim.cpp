@@ -97,4 +97,39 @@ int dropin_run(int engine, const float* tree_src, std::size_t w, std::size_t h, 
   return 0;
 }
 
+// RiemersmaBlocksCuda's fused forms: `in_raw` (the decoder's frames, used
+// when upload) read per in_mode / in_channels, `batch` RgbaF (used when not
+// upload, and as the output when not emit), `out_raw` rgba64 or planar 4:4:4.
+int dropin_blocks_fused(const float* tree_src, std::size_t w, std::size_t h, int colors,
+                        int assoc, float* batch, int frames, int block, int upload, int in_mode,
+                        int in_channels, const void* in_raw, int emit, int emit_yuv444,
+                        void* out_raw, char* err, std::size_t errlen) {
+  rd::ColorTree tree;
+  tree.Build(reinterpret_cast<const rd::RgbaF*>(tree_src), w, h, colors, assoc != 0, false);
+  static rd::Palette pal;
+  pal = rd::Palette();
+  pal.count = tree.color_count();
+  pal.associate_alpha = assoc != 0;
+  for (int i = 0; i < pal.count; ++i) pal.entries[i] = tree.colormap()[i];
+  rd::DitherParams p;
+  p.colors = colors;
+  rd::BlockOptions o;
+  o.block = block;
+  o.frames = frames;
+  o.upload_u16 = upload != 0;
+  o.in_mode = static_cast<rd::BlockOptions::InMode>(in_mode);
+  o.in_channels = in_channels;
+  o.emit_u16 = emit != 0;
+  o.emit_yuv444 = emit_yuv444 != 0;
+  std::string name;
+  const std::string e = rd::RiemersmaBlocksCuda(
+      pal, p, tree, w, h, reinterpret_cast<rd::RgbaF*>(batch), o, &name,
+      static_cast<std::uint16_t*>(out_raw), 0, static_cast<const std::uint16_t*>(in_raw));
+  if (!e.empty()) {
+    Copy(e, err, errlen);
+    return -1;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -649,3 +649,131 @@ void orc_inverse_filter(int taps, double diffusion, double* g) {
     g[d] = acc;
   }
 }
+
+/* ---- video frame formats on either side of the block walk ----------------
+ * RiemersmaBlocksCpu's fused gather widens the decoder's bytes to the RgbaF a
+ * reader would have produced, and its fused output is the convert pass's
+ * arithmetic applied to the RgbaF the non-fused walk leaves behind
+ * (src/rd_riemersma_cpu.cpp:711-753 says so and reproduces it byte for byte),
+ * so the checker is widen -> orc_walk_blocks -> narrow. */
+
+/* include/rd_types.h:75-97 (SwsClip16, SwsYuvToRgb16), in the reference's
+ * own order of operations: unsigned wrap of (c - 128) * 512, the 0x10000 and
+ * -8192 luma offsets, the 9539 scale, the (1 << 13) - (1 << 29) rounding
+ * offset, >> 14, clip around 1 << 15. */
+static uint16_t sws_clip(int x) {
+  const int v = x + 32768;
+  return (uint16_t)(v < 0 ? 0 : (v > 65535 ? 65535 : v));
+}
+static void sws_yuv_to_rgb16(unsigned y, unsigned u, unsigned v, uint16_t out[3]) {
+  int yy = (int)((y - 128u) * 512u);
+  const int uu = (int)((u - 128u) * 512u);
+  const int vv = (int)((v - 128u) * 512u);
+  yy += 0x10000;
+  yy -= 8192;
+  yy *= 9539;
+  yy += (1 << 13) - (1 << 29);
+  out[0] = sws_clip((vv * 13075 + yy) >> 14);
+  out[1] = sws_clip((vv * -6660 + uu * -3209 + yy) >> 14);
+  out[2] = sws_clip((uu * 16525 + yy) >> 14);
+}
+
+/* src/rd_blocks_cuda.cu:660-676 (d_chroma_bilinear) as the 4:2:0 gather calls
+ * it (:677-706): chroma plane w2 x h2, sample (x >> 1, y >> 1), phase (x & 1,
+ * y & 1).  The reference has no CPU form of this mode. */
+static unsigned chroma_bilinear(const unsigned char* plane, int w2, int h2, int x, int y) {
+  const int cx = x >> 1, cy = y >> 1, ox = x & 1, oy = y & 1;
+  const int x1 = (cx + 1 < w2) ? cx + 1 : cx;
+  const int y1 = (cy + 1 < h2) ? cy + 1 : cy;
+  const int a = plane[(size_t)cy * w2 + cx];
+  const int b = plane[(size_t)cy * w2 + x1];
+  const int c = plane[(size_t)y1 * w2 + cx];
+  const int d = plane[(size_t)y1 * w2 + x1];
+  const int top = a * (2 - ox) + b * ox;
+  const int bot = c * (2 - ox) + d * ox;
+  return (unsigned)((top * (2 - oy) + bot * oy + 2) >> 2);
+}
+
+/* src/rd_riemersma_cpu.cpp:496-516 (gather_pixel) for formats 6 (rgb48),
+ * 8 (rgba64) and 444 (planar 4:4:4); 420 (planar 4:2:0) per the CUDA gather
+ * above; 3 / 4 / 16 as the reader gives them (8-bit samples x 257, RgbaF as
+ * is).  Writes W*H RgbaF. Returns -1 for an unknown format or odd 4:2:0. */
+int orc_widen_frame(int format, const void* in, size_t width, size_t height, float* rgba) {
+  const size_t n = width * height;
+  const unsigned char* b = (const unsigned char*)in;
+  const uint16_t* q = (const uint16_t*)in;
+  if (format == 420 && ((width & 1) || (height & 1))) return -1;
+  for (size_t p = 0; p < n; ++p) {
+    float* o = rgba + 4 * p;
+    switch (format) {
+      case 3:
+        o[0] = (float)(b[3 * p] * 257); o[1] = (float)(b[3 * p + 1] * 257);
+        o[2] = (float)(b[3 * p + 2] * 257); o[3] = 65535.0f;
+        break;
+      case 4:
+        o[0] = (float)(b[4 * p] * 257); o[1] = (float)(b[4 * p + 1] * 257);
+        o[2] = (float)(b[4 * p + 2] * 257); o[3] = (float)(b[4 * p + 3] * 257);
+        break;
+      case 16:
+        memcpy(o, (const float*)in + 4 * p, 16);
+        break;
+      case 6:
+        o[0] = (float)q[3 * p]; o[1] = (float)q[3 * p + 1]; o[2] = (float)q[3 * p + 2];
+        o[3] = (float)65535.0;
+        break;
+      case 8:
+        o[0] = (float)q[4 * p]; o[1] = (float)q[4 * p + 1]; o[2] = (float)q[4 * p + 2];
+        o[3] = (float)q[4 * p + 3];
+        break;
+      case 444:
+      case 420: {
+        uint16_t rgb[3];
+        unsigned u, v;
+        if (format == 444) {
+          u = b[n + p];
+          v = b[2 * n + p];
+        } else {
+          const int w2 = (int)(width >> 1), h2 = (int)(height >> 1);
+          const int x = (int)(p % width), y = (int)(p / width);
+          u = chroma_bilinear(b + n, w2, h2, x, y);
+          v = chroma_bilinear(b + n + (size_t)w2 * h2, w2, h2, x, y);
+        }
+        sws_yuv_to_rgb16(b[p], u, v, rgb);
+        o[0] = (float)rgb[0]; o[1] = (float)rgb[1]; o[2] = (float)rgb[2];
+        o[3] = (float)65535.0;
+        break;
+      }
+      default:
+        return -1;
+    }
+  }
+  return 0;
+}
+
+/* The convert pass the fused output replaces: FloatsToRaw's four uint16 per
+ * pixel (format 8) or FloatsToYuv444's planar BT.601 bytes (format 444), as
+ * src/rd_riemersma_cpu.cpp:719-753 and :776-801 restate them: (int)float >> 8
+ * per channel, then ((66r + 129g + 25b + 128) >> 8) + 16 and the two chroma
+ * rows, clamped to a byte.  Returns -1 for an unknown format. */
+int orc_narrow_frame(int format, const float* rgba, size_t width, size_t height, void* out) {
+  const size_t n = width * height;
+  for (size_t p = 0; p < n; ++p) {
+    const float* s = rgba + 4 * p;
+    if (format == 8) {
+      uint16_t* u = (uint16_t*)out + 4 * p;
+      u[0] = (uint16_t)s[0]; u[1] = (uint16_t)s[1]; u[2] = (uint16_t)s[2]; u[3] = (uint16_t)s[3];
+    } else if (format == 444) {
+      unsigned char* o = (unsigned char*)out;
+      const int r8 = (int)s[0] >> 8, g8 = (int)s[1] >> 8, b8 = (int)s[2] >> 8;
+      const int yv = ((66 * r8 + 129 * g8 + 25 * b8 + 128) >> 8) + 16;
+      const int uv = ((-38 * r8 - 74 * g8 + 112 * b8 + 128) >> 8) + 128;
+      const int vv = ((112 * r8 - 94 * g8 - 18 * b8 + 128) >> 8) + 128;
+      o[p] = (unsigned char)(yv < 0 ? 0 : (yv > 255 ? 255 : yv));
+      o[n + p] = (unsigned char)(uv < 0 ? 0 : (uv > 255 ? 255 : uv));
+      o[2 * n + p] = (unsigned char)(vv < 0 ? 0 : (vv > 255 ? 255 : vv));
+    } else {
+      return -1;
+    }
+  }
+  return 0;
+}

@@ -96,6 +96,15 @@ int orc_walk_blocks(const orc_tree* t, const orc_entry* palette, int count,
                     int associate_alpha, double diffusion, int block,
                     size_t width, size_t height, float* pixels, uint8_t* idx_out);
 
+/* Video frame formats (codes as the library's RDB_* formats: 3 RGB8, 4 RGBA8,
+ * 16 RgbaF, 6 rgb48, 8 rgba64, 444 planar 4:4:4, 420 planar 4:2:0).
+ * orc_widen_frame: src/rd_riemersma_cpu.cpp:496-516 (gather_pixel),
+ * include/rd_types.h:75-97, and src/rd_blocks_cuda.cu:660-706 for 4:2:0.
+ * orc_narrow_frame (formats 8 and 444): src/rd_riemersma_cpu.cpp:719-753.
+ * Both return -1 on an unknown format. */
+int orc_widen_frame(int format, const void* in, size_t width, size_t height, float* rgba);
+int orc_narrow_frame(int format, const float* rgba, size_t width, size_t height, void* out);
+
 /* src/rd_approx_cuda.cu:73-88 (BuildInverseFilter). g has taps+1 entries. */
 void orc_inverse_filter(int taps, double diffusion, double* g);
 

@@ -106,6 +106,10 @@ class Oracle:
         lib.orc_tree_lookup.argtypes = [C.POINTER(OrcTree), C.c_double, C.c_double, C.c_double,
                                         C.c_double]
         lib.orc_tree_lookup.restype = C.c_int
+        lib.orc_widen_frame.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_size_t, _f32p]
+        lib.orc_widen_frame.restype = C.c_int
+        lib.orc_narrow_frame.argtypes = [C.c_int, _f32p, C.c_size_t, C.c_size_t, C.c_void_p]
+        lib.orc_narrow_frame.restype = C.c_int
 
     # -- palette -------------------------------------------------------------
     def build_tree_raw(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool):
@@ -192,36 +196,50 @@ class Oracle:
         n = self.lib.orc_seq_order(w, h, out)
         return out[:n]
 
-    def walk_seq_frame(self, tree_src: np.ndarray, frame: np.ndarray, max_colors: int,
-                       assoc: bool, gray: bool, diffusion: float = 1.0,
-                       use_cache: bool = True) -> np.ndarray:
-        """RiemersmaWalkCpu of `frame` with the tree built from `tree_src`."""
-        h, w = tree_src.shape[:2]
-        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
-        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), int(gray))
-        try:
-            out = np.ascontiguousarray(frame, dtype=np.float32).reshape(-1).copy()
-            self.lib.ref_walk_seq(t, float(diffusion), int(use_cache), w, h, out)
-            return out.reshape(h, w, 4)
-        finally:
-            self.lib.ref_tree_free(t)
+    # -- video frame formats ---------------------------------------------------
+    def widen_frame(self, fmt: int, raw, w: int, h: int) -> np.ndarray:
+        """orc_widen_frame: one frame of `fmt` bytes -> (h, w, 4) RgbaF."""
+        buf = np.ascontiguousarray(np.frombuffer(np.ascontiguousarray(raw).tobytes(), np.uint8))
+        out = np.empty(w * h * 4, np.float32)
+        if self.lib.orc_widen_frame(int(fmt), buf.ctypes.data, w, h, out) != 0:
+            raise ValueError(f"format {fmt} not widened")
+        return out.reshape(h, w, 4)
 
-    def walk_blocks_frames(self, tree_src: np.ndarray, frames: np.ndarray, max_colors: int,
-                           assoc: bool, gray: bool, block: int, diffusion: float = 1.0):
-        """RiemersmaBlocksCpu over F frames in place ((F, H, W, 4) float32), the
-        tree built from `tree_src`.  Returns (0, "") or (-1, refusal)."""
-        h, w = tree_src.shape[:2]
-        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
-        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), int(gray))
+    def narrow_frame(self, fmt: int, rgbaf: np.ndarray) -> np.ndarray:
+        """orc_narrow_frame: (h, w, 4) RgbaF -> the frame's bytes as uint8."""
+        h, w = rgbaf.shape[:2]
+        src = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1)
+        out = np.zeros(w * h * (8 if fmt == 8 else 3), np.uint8)
+        if self.lib.orc_narrow_frame(int(fmt), src, w, h, out.ctypes.data) != 0:
+            raise ValueError(f"format {fmt} not narrowed")
+        return out
+
+    def walk_blocks_raw(self, tree_src: np.ndarray, raw_frames: np.ndarray, in_fmt: int,
+                        w: int, h: int, out_fmt: int, max_colors: int, assoc: bool,
+                        block: int, diffusion: float = 1.0):
+        """RiemersmaBlocksCpu's fused form restated: every frame (one row of
+        `raw_frames`, uint8) is widened, block-walked with the tree built from
+        `tree_src` (RgbaF) and narrowed to `out_fmt` (16 = RgbaF bytes).
+        Returns (out (F, bytes) uint8, indices (F, h, w))."""
+        t = self.build_tree_raw(tree_src, max_colors, assoc, False)
         try:
-            flat = frames.reshape(-1)
-            assert flat.base is frames or flat.base is frames.base or np.shares_memory(flat, frames)
-            err = C.create_string_buffer(1024)
-            rc = self.lib.ref_walk_blocks(t, float(diffusion), int(block), w, h, flat,
-                                          frames.shape[0], err, 1024)
-            return rc, err.value.decode()
+            count = t.color_count
+            pal = np.ctypeslib.as_array(t.colormap, shape=(max(count, 1) * 4,)).copy()
+            outs, idxs = [], []
+            for f in range(raw_frames.shape[0]):
+                px = self.widen_frame(in_fmt, raw_frames[f], w, h).reshape(-1).copy()
+                idx = np.zeros(w * h, np.uint8)
+                rc = self.lib.orc_walk_blocks(C.byref(t), pal, count, int(assoc),
+                                              float(diffusion), int(block), w, h, px, idx)
+                if rc != 0:
+                    raise ValueError("blocks walk refused")
+                px = px.reshape(h, w, 4)
+                outs.append(px.view(np.uint8).reshape(-1) if out_fmt == 16
+                            else self.narrow_frame(out_fmt, px))
+                idxs.append(idx.reshape(h, w))
+            return np.stack(outs), np.stack(idxs)
         finally:
-            self.lib.ref_tree_free(t)
+            self.lib.orc_tree_free(C.byref(t))
 
     def block_order(self, w: int, h: int):
         out = np.empty(w * h + 1, np.int32)
@@ -261,6 +279,11 @@ class RefLib:
         lib.ref_walk_blocks.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_size_t, C.c_size_t,
                                         _f32p, C.c_int, C.c_char_p, C.c_size_t]
         lib.ref_walk_blocks.restype = C.c_int
+        lib.ref_walk_blocks_raw.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_size_t,
+                                            C.c_size_t, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                            C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_char_p,
+                                            C.c_size_t]
+        lib.ref_walk_blocks_raw.restype = C.c_int
         lib.ref_hilbert_point.argtypes = [C.c_int64, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.ref_curve_level.argtypes = [C.c_size_t, C.c_size_t]
         lib.ref_block_curve.argtypes = [C.c_size_t, C.c_size_t, _i32p, _i32p]
@@ -361,6 +384,35 @@ class RefLib:
         finally:
             self.lib.ref_tree_free(t)
 
+    def walk_blocks_raw(self, tree_src: np.ndarray, in_frames, gather_layout: int,
+                        gather_channels: int, w: int, h: int, out_yuv444: bool,
+                        max_colors: int, assoc: bool, block: int, diffusion: float = 1.0):
+        """RiemersmaBlocksCpu's fused output (and, with gather_layout 3 or 4,
+        fused gather) over F frames, the tree built from `tree_src`.
+        `in_frames`: (F, H, W, 4) float32 when gather_layout is 0, else (F,
+        frame_bytes) uint8 of the decoder's bytes.  Returns (rc, message,
+        out (F, bytes) uint8)."""
+        src = np.ascontiguousarray(tree_src, dtype=np.float32).reshape(-1)
+        t = self.lib.ref_tree_build(src, w, h, int(max_colors), int(assoc), 0)
+        try:
+            frames = in_frames.shape[0]
+            out = np.zeros((frames, w * h * (3 if out_yuv444 else 8)), np.uint8)
+            err = C.create_string_buffer(1024)
+            if gather_layout == 0:
+                rgba = np.ascontiguousarray(in_frames, dtype=np.float32)
+                rc = self.lib.ref_walk_blocks_raw(t, float(diffusion), int(block), w, h,
+                                                  rgba.ctypes.data, frames, out.ctypes.data,
+                                                  int(out_yuv444), None, 0, 0, 0, err, 1024)
+            else:
+                raw = np.ascontiguousarray(in_frames, dtype=np.uint8)
+                rc = self.lib.ref_walk_blocks_raw(t, float(diffusion), int(block), w, h, None,
+                                                  frames, out.ctypes.data, int(out_yuv444),
+                                                  raw.ctypes.data, raw.shape[1], int(gather_layout),
+                                                  int(gather_channels), err, 1024)
+            return rc, err.value.decode(), out
+        finally:
+            self.lib.ref_tree_free(t)
+
     def block_order(self, w: int, h: int):
         out = np.empty(w * h + 1, np.int32)
         owner = np.empty(max(w * h, 1), np.int32)
@@ -407,6 +459,11 @@ class DropinLib:
                                    f32, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_int, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
         lib.dropin_run.restype = C.c_int
+        lib.dropin_blocks_fused.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_int, C.c_int,
+                                            C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                            C.c_char_p, C.c_size_t]
+        lib.dropin_blocks_fused.restype = C.c_int
 
     def run(self, engine: str, tree_src: np.ndarray, frames: np.ndarray, colors: int,
             assoc: bool = False, gray: bool = False, diffusion: float = 1.0,
@@ -422,6 +479,22 @@ class DropinLib:
                                  frames, frames.shape[0], float(diffusion), int(use_cache), block,
                                  iterations, taps, slot, err, 512, dev, 256)
         return ("" if rc == 0 else err.value.decode()), dev.value.decode()
+
+    def blocks_fused(self, tree_src: np.ndarray, frames: int, colors: int, assoc: bool = False,
+                     block: int = 512, batch: np.ndarray | None = None, in_raw=None,
+                     in_mode: int = 0, in_channels: int = 4, out_raw=None,
+                     emit_yuv444: bool = False) -> str:
+        """RiemersmaBlocksCuda with upload_u16 (when in_raw is given) and / or
+        emit_u16 (when out_raw is given).  Returns the error or ""."""
+        h, w = tree_src.shape[:2]
+        err = C.create_string_buffer(512)
+        src = np.ascontiguousarray(tree_src, np.float32)
+        ptr = (lambda a: None if a is None else a.ctypes.data)
+        rc = self.lib.dropin_blocks_fused(
+            src.ctypes.data, w, h, colors, int(assoc), ptr(batch), frames, block,
+            int(in_raw is not None), in_mode, in_channels, ptr(in_raw), int(out_raw is not None),
+            int(emit_yuv444), ptr(out_raw), err, 512)
+        return "" if rc == 0 else err.value.decode()
 
     def inverse_filter(self, taps: int, diffusion: float = 1.0) -> np.ndarray:
         out = np.zeros(taps + 1, np.float64)

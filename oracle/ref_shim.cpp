@@ -101,6 +101,33 @@ int ref_walk_blocks(void* h, double diffusion, int block, std::size_t w, std::si
   return 0;
 }
 
+// RiemersmaBlocksCpu with its fused gather and output (src/rd_riemersma_cpu.cpp:
+// 224-268, 489-516, 711-801).  `rgba` is read when gather_layout is 0 (and is
+// then left unwritten); gather_layout 3 = planar 8-bit 4:4:4, 4 = interleaved
+// uint16 with gather_channels 3 or 4.  raw_out receives rgba64 (out_yuv444 0)
+// or planar 4:4:4 bytes per frame.
+int ref_walk_blocks_raw(void* h, double diffusion, int block, std::size_t w, std::size_t hgt,
+                        float* rgba, int frames, unsigned char* raw_out, int out_yuv444,
+                        const unsigned char* gather_raw, std::size_t gather_frame_bytes,
+                        int gather_layout, int gather_channels, char* err, std::size_t errlen) {
+  RefTree* t = static_cast<RefTree*>(h);
+  rd::DitherParams p;
+  p.diffusion = diffusion;
+  p.use_cache = false;
+  std::string e;
+  rd::RiemersmaBlocksCpu(*t->palette, p, t->tree, w, hgt, reinterpret_cast<rd::RgbaF*>(rgba),
+                         frames, block, raw_out, w * hgt, out_yuv444 != 0, &e, gather_raw,
+                         gather_frame_bytes, gather_layout, gather_channels);
+  if (!e.empty()) {
+    if (err && errlen) {
+      std::strncpy(err, e.c_str(), errlen - 1);
+      err[errlen - 1] = '\0';
+    }
+    return -1;
+  }
+  return 0;
+}
+
 void ref_hilbert_point(int64_t n, int level, int* x, int* y) { rd::HilbertPoint(n, level, x, y); }
 
 int ref_curve_level(std::size_t w, std::size_t h) { return rd::ComputeCurveLevel(w, h); }

@@ -97,6 +97,27 @@ class Job(C.Structure):
 
 HostJob = Job  # same layout: rdb_host_job
 
+# Frame formats of rdb_dither_frames (include/rdb.h), beside RGB8 / RGBA8 /
+# RGBAF32 = 3 / 4 / 16.
+RGB8, RGBA8, RGBAF32 = 3, 4, 16
+RGB16, RGBA16, YUV444P8, YUV420P8 = 6, 8, 444, 420
+
+
+class Frames(C.Structure):
+    _fields_ = [
+        ("inp", C.c_void_p),
+        ("in_frame_bytes", C.c_size_t),
+        ("in_format", C.c_int),
+        ("width", C.c_int),
+        ("height", C.c_int),
+        ("frames", C.c_int),
+        ("palette_id", C.c_int),
+        ("out_format", C.c_int),
+        ("out", C.c_void_p),
+        ("out_frame_bytes", C.c_size_t),
+        ("indices", C.c_void_p),
+    ]
+
 
 class PaletteDesc(C.Structure):
     _fields_ = [
@@ -153,6 +174,9 @@ SIGNATURES = {
     "rdb_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rdb_dither_host": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(HostJob), C.c_int,
                                   C.POINTER(Options)]),
+    "rdb_frame_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    "rdb_dither_frames": (C.c_int, [C.c_void_p, C.POINTER(Frames), C.POINTER(Options), C.c_void_p]),
+    "rdb_dither_frames_host": (C.c_int, [C.c_void_p, C.POINTER(Frames), C.POINTER(Options)]),
     "rdb_dither_seq_noalloc": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int,
                                          C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_int,
                                          C.c_void_p]),
@@ -378,6 +402,59 @@ class Context:
         o = options(**opts)
         _check(load().rdb_dither_host(self.handle, eng, C.byref(job), 1, C.byref(o)))
 
+    def dither_frames_host(self, frames, in_format: int, width: int, height: int,
+                           palette_id: int, out_format: int, indices: bool = False,
+                           out=None, **opts):
+        """Video frames through the blocks engine (rdb_dither_frames_host):
+        `frames` holds F packed frames of `in_format` (any array whose bytes
+        are F * frame_bytes(in_format)); returns the F output frames as a
+        uint8 array (F, frame_bytes(out_format)) -- or fills `out` -- and,
+        with indices=True, the (F, height, width) index maps."""
+        buf = np.ascontiguousarray(frames)
+        in_bytes = frame_bytes(in_format, width, height)
+        out_bytes = frame_bytes(out_format, width, height)
+        if in_bytes == 0 or out_bytes == 0 or buf.nbytes % in_bytes:
+            raise ValueError("frames do not hold whole frames of the format")
+        nf = buf.nbytes // in_bytes
+        if out is None:
+            out = np.zeros((nf, out_bytes), np.uint8)
+        elif out.nbytes != nf * out_bytes or not out.flags.c_contiguous:
+            raise ValueError("out must be contiguous and hold every output frame")
+        f = Frames()
+        f.inp = _ptr(buf)
+        f.in_format = in_format
+        f.width = width
+        f.height = height
+        f.frames = nf
+        f.palette_id = palette_id
+        f.out_format = out_format
+        f.out = _ptr(out)
+        idx = np.zeros((nf, height, width), np.uint8) if indices else None
+        f.indices = _ptr(idx) if indices else 0
+        o = options(**opts)
+        _check(load().rdb_dither_frames_host(self.handle, C.byref(f), C.byref(o)))
+        return (out, idx) if indices else out
+
+    def dither_frames(self, inp: int, in_format: int, width: int, height: int, frames: int,
+                      palette_id: int, out: int, out_format: int, indices: int = 0,
+                      in_frame_bytes: int = 0, out_frame_bytes: int = 0,
+                      stream: int | None = None, **opts) -> None:
+        """Device-pointer form (rdb_dither_frames), asynchronous on `stream`."""
+        f = Frames()
+        f.inp = inp
+        f.in_frame_bytes = in_frame_bytes
+        f.in_format = in_format
+        f.width = width
+        f.height = height
+        f.frames = frames
+        f.palette_id = palette_id
+        f.out_format = out_format
+        f.out = out
+        f.out_frame_bytes = out_frame_bytes
+        f.indices = indices
+        o = options(**opts)
+        _check(load().rdb_dither_frames(self.handle, C.byref(f), C.byref(o), stream or None))
+
     # -- dithering (device buffers; torch tensors as plumbing) ------------
     def dither(self, engine: str | int, jobs: list[dict], stream: int | None = None,
                **opts) -> None:
@@ -461,6 +538,11 @@ def inverse_filter(taps: int, diffusion: float = 1.0) -> np.ndarray:
     g = np.zeros(taps + 1, np.float64)
     _check(load().rdb_inverse_filter(taps, diffusion, _ptr(g)))
     return g
+
+
+def frame_bytes(fmt: int, width: int, height: int) -> int:
+    """Bytes of one packed frame of `fmt` (0 when unknown or invalid)."""
+    return int(load().rdb_frame_bytes(fmt, width, height))
 
 
 def block_gap(width: int, height: int) -> int:

@@ -320,6 +320,25 @@ int rdb_dither_host(rdb_context* ctx, int engine, const rdb_host_job* jobs, int 
   return ctx->impl.DitherHost(engine, jobs, n_jobs, o);
 }
 
+size_t rdb_frame_bytes(int format, int width, int height) {
+  return rdb::FrameBytes(format, width, height);
+}
+
+int rdb_dither_frames(rdb_context* ctx, const rdb_frames* f, const rdb_options* opts,
+                      void* stream) {
+  if (!ctx || !f) return Guard("rdb_dither_frames");
+  rdb_options o;
+  if (opts) o = *opts; else rdb_options_default(&o);
+  return ctx->impl.Frames(*f, o, static_cast<cudaStream_t>(stream));
+}
+
+int rdb_dither_frames_host(rdb_context* ctx, const rdb_frames* f, const rdb_options* opts) {
+  if (!ctx || !f) return Guard("rdb_dither_frames_host");
+  rdb_options o;
+  if (opts) o = *opts; else rdb_options_default(&o);
+  return ctx->impl.FramesHost(*f, o);
+}
+
 void rdb_error_weights(double out[16]) {
   if (out) rdb::error_weights(out);
 }

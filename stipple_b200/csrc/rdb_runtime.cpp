@@ -514,9 +514,6 @@ int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t 
 }
 
 int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
-  if (o.block < kQueue) {
-    return Fail(RDB_E_UNSUPPORTED, "--blocks must be at least 16 (the error queue is 16 entries deep)");
-  }
   const int pid = jobs[0].palette_id;
   const int layout = jobs[0].layout;
   for (int i = 1; i < n; ++i) {
@@ -524,36 +521,44 @@ int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream
       return Fail(RDB_E_INVALID, "blocks engine: one palette and one layout per call");
     }
   }
-  const DevPlan* p = Plan(pid);
-  std::vector<BlockImage> imgs;
-  std::vector<int64_t> offs;
-  int64_t blocks = 0, positions = 0;
+  std::vector<BlockImage> imgs(static_cast<std::size_t>(n));
   for (int i = 0; i < n; ++i) {
     const rdb_job& j = jobs[i];
-    const int64_t nb = BlockListLength(j.width, j.height);
-    if (nb == 0) {
-      // 1x1: BuildCurveIndex is empty and the pixel keeps its value.
-      if (j.rgba_out && j.rgba_out != j.pixels) {
-        const cudaError_t e = LaunchCopySource(static_cast<const unsigned char*>(j.pixels),
-                                               static_cast<int64_t>(RowStride(j)), j.width,
-                                               j.height, j.layout,
-                                               reinterpret_cast<float4*>(j.rgba_out), s);
-        if (e != cudaSuccess) return CudaFail(e, "source copy");
-      }
-      continue;
-    }
-    const int32_t* order = nullptr;
-    if (int rc = Order(j.width, j.height, s, &order)) return rc;
-    BlockImage b{};
+    BlockImage& b = imgs[static_cast<std::size_t>(i)];
     b.pixels = static_cast<const unsigned char*>(j.pixels);
     b.row_stride = static_cast<int64_t>(RowStride(j));
     b.width = j.width;
     b.height = j.height;
     b.layout = j.layout;
-    b.n = static_cast<int>(nb);
-    b.order = order;
     b.indices = j.indices;
+    // An RgbaF input dithered in place already holds its source values.
     b.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+    if (j.rgba_out == j.pixels && BlockListLength(j.width, j.height) == 0) b.rgba_out = nullptr;
+  }
+  return RunBlocks(pid, layout, imgs, o, s);
+}
+
+// Shared by rdb_dither's blocks engine and the video-frame form: `imgs` hold
+// everything but the walk bookkeeping, which is filled in here.
+int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const rdb_options& o,
+                       cudaStream_t s) {
+  if (o.block < kQueue) {
+    return Fail(RDB_E_UNSUPPORTED, "--blocks must be at least 16 (the error queue is 16 entries deep)");
+  }
+  const DevPlan* p = Plan(pid);
+  std::vector<BlockImage> imgs;
+  std::vector<int64_t> offs;
+  int64_t blocks = 0, positions = 0;
+  for (BlockImage b : all) {
+    const int64_t nb = BlockListLength(b.width, b.height);
+    if (nb == 0) {
+      // 1x1: BuildCurveIndex is empty and the pixel keeps its value.
+      const cudaError_t e = LaunchSourceFill(b, s);
+      if (e != cudaSuccess) return CudaFail(e, "source copy");
+      continue;
+    }
+    if (int rc = Order(b.width, b.height, s, &b.order)) return rc;
+    b.n = static_cast<int>(nb);
     b.first_block = blocks;
     b.nblocks = static_cast<int>((nb + o.block - 1) / o.block);
     blocks += b.nblocks;
@@ -562,7 +567,8 @@ int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream
     imgs.push_back(b);
   }
   if (imgs.empty()) return RDB_OK;
-  const std::size_t word = layout == RDB_RGBAF32 ? 16 : 4;
+  const bool packed = layout == RDB_RGB8 || layout == RDB_RGBA8;
+  const std::size_t word = packed ? 4 : 16;
   if (int rc = Reserve(&block_images_, imgs.size() * sizeof(BlockImage), "block images")) return rc;
   if (int rc = Reserve(&block_offsets_, offs.size() * sizeof(int64_t), "block offsets")) return rc;
   if (int rc = Reserve(&block_cx_, static_cast<std::size_t>(positions) * word, "block samples")) return rc;
@@ -584,12 +590,165 @@ int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream
   L.plan = p->dev;
   L.plan_smem = p->smem;
   L.assoc = p->assoc ? 1 : 0;
-  L.is_float = layout == RDB_RGBAF32 ? 1 : 0;
+  L.is_float = packed ? 0 : 1;
   scaled_weights(o.diffusion, L.sw);
   L.status = static_cast<int*>(status_.ptr);
   e = LaunchBlockWalk(L, positions, s);
   if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
   return RDB_OK;
+}
+
+std::size_t FrameBytes(int format, int width, int height) {
+  if (width < 1 || height < 1) return 0;
+  const std::size_t px = static_cast<std::size_t>(width) * static_cast<std::size_t>(height);
+  switch (format) {
+    case RDB_RGB8: return px * 3;
+    case RDB_RGBA8: return px * 4;
+    case RDB_RGBAF32: return px * 16;
+    case RDB_RGB16: return px * 6;
+    case RDB_RGBA16: return px * 8;
+    case RDB_YUV444P8: return px * 3;
+    case RDB_YUV420P8: return (width % 2 || height % 2) ? 0 : px * 3 / 2;
+    default: return 0;
+  }
+}
+
+int Context::CheckFrames(const rdb_frames& f) const {
+  if (f.width < 1 || f.height < 1 || f.frames < 1) {
+    return Fail(RDB_E_INVALID, "frames must be at least 1x1 and at least one");
+  }
+  if (static_cast<int64_t>(f.width) * f.height >= (static_cast<int64_t>(1) << 31) - 1) {
+    return Fail(RDB_E_UNSUPPORTED, "frame larger than 2^31 - 2 pixels");
+  }
+  if (!f.in || !f.out) return Fail(RDB_E_INVALID, "null frame buffer");
+  const std::size_t in_bytes = FrameBytes(f.in_format, f.width, f.height);
+  if (!in_bytes) {
+    return Fail(RDB_E_INVALID, f.in_format == RDB_YUV420P8
+                                   ? "4:2:0 frames must have even width and height"
+                                   : "unknown input frame format");
+  }
+  if (f.out_format != RDB_RGBA16 && f.out_format != RDB_YUV444P8 && f.out_format != RDB_RGBAF32) {
+    return Fail(RDB_E_INVALID, "output frame format must be RGBA16, YUV444P8 or RGBAF32");
+  }
+  const std::size_t out_bytes = FrameBytes(f.out_format, f.width, f.height);
+  const std::size_t in_pitch = f.in_frame_bytes ? f.in_frame_bytes : in_bytes;
+  const std::size_t out_pitch = f.out_frame_bytes ? f.out_frame_bytes : out_bytes;
+  if (in_pitch < in_bytes || out_pitch < out_bytes) {
+    return Fail(RDB_E_INVALID, "frame stride shorter than a frame");
+  }
+  // Vector loads and stores: float4 (16), ushort4 / RGBA8 words (8 / 4),
+  // uint16 channels (2).
+  const auto align = [](int fmt) -> std::size_t {
+    switch (fmt) {
+      case RDB_RGBAF32: return 16;
+      case RDB_RGBA16: return 8;
+      case RDB_RGBA8: return 4;
+      case RDB_RGB16: return 2;
+      default: return 1;
+    }
+  };
+  const std::size_t ai = align(f.in_format), ao = align(f.out_format);
+  if ((reinterpret_cast<uintptr_t>(f.in) | in_pitch) % ai ||
+      (reinterpret_cast<uintptr_t>(f.out) | out_pitch) % ao) {
+    return Fail(RDB_E_INVALID, "frame buffer or stride breaks the format's alignment");
+  }
+  if (f.in == f.out && !(f.in_format == RDB_RGBAF32 && f.out_format == RDB_RGBAF32 &&
+                         in_pitch == out_pitch)) {
+    return Fail(RDB_E_INVALID, "only RGBAF32 frames may be dithered in place");
+  }
+  const DevPlan* p = Plan(f.palette_id);
+  if (!p) return Fail(RDB_E_INVALID, "unknown palette id");
+  return RDB_OK;
+}
+
+int Context::Frames(const rdb_frames& f, const rdb_options& o, cudaStream_t s) {
+  if (int rc = CheckFrames(f)) return rc;
+  if (!s) s = stream_;
+  cudaSetDevice(device_);
+  if (!scratch_ev_) {
+    const cudaError_t e = cudaEventCreateWithFlags(&scratch_ev_, cudaEventDisableTiming);
+    if (e != cudaSuccess) return CudaFail(e, "scratch event");
+  } else if (scratch_stream_ != s) {
+    cudaStreamWaitEvent(s, scratch_ev_, 0);
+  }
+  const std::size_t in_pitch =
+      f.in_frame_bytes ? f.in_frame_bytes : FrameBytes(f.in_format, f.width, f.height);
+  const std::size_t out_pitch =
+      f.out_frame_bytes ? f.out_frame_bytes : FrameBytes(f.out_format, f.width, f.height);
+  const std::size_t npx = static_cast<std::size_t>(f.width) * f.height;
+  const bool planar = f.in_format == RDB_YUV444P8 || f.in_format == RDB_YUV420P8;
+  std::vector<BlockImage> imgs(static_cast<std::size_t>(f.frames));
+  for (int k = 0; k < f.frames; ++k) {
+    BlockImage& b = imgs[static_cast<std::size_t>(k)];
+    b.pixels = static_cast<const unsigned char*>(f.in) + static_cast<std::size_t>(k) * in_pitch;
+    b.row_stride = planar ? f.width
+                          : static_cast<int64_t>(FrameBytes(f.in_format, f.width, 1));
+    b.width = f.width;
+    b.height = f.height;
+    b.layout = f.in_format;
+    b.indices = f.indices ? f.indices + static_cast<std::size_t>(k) * npx : nullptr;
+    unsigned char* out = static_cast<unsigned char*>(f.out) + static_cast<std::size_t>(k) * out_pitch;
+    if (f.out_format == RDB_RGBAF32) {
+      b.rgba_out = (out == b.pixels && BlockListLength(f.width, f.height) == 0)
+                       ? nullptr
+                       : reinterpret_cast<float4*>(out);
+    } else {
+      b.raw_out = out;
+      b.out_format = f.out_format;
+    }
+  }
+  const int rc = RunBlocks(f.palette_id, f.in_format, imgs, o, s);
+  cudaEventRecord(scratch_ev_, s);
+  scratch_stream_ = s;
+  return rc;
+}
+
+int Context::FramesHost(const rdb_frames& f, const rdb_options& o) {
+  if (int rc = CheckFrames(f)) return rc;
+  const std::size_t in_bytes = FrameBytes(f.in_format, f.width, f.height);
+  const std::size_t out_bytes = FrameBytes(f.out_format, f.width, f.height);
+  const std::size_t in_pitch = f.in_frame_bytes ? f.in_frame_bytes : in_bytes;
+  const std::size_t out_pitch = f.out_frame_bytes ? f.out_frame_bytes : out_bytes;
+  const std::size_t frames = static_cast<std::size_t>(f.frames);
+  const std::size_t npx = static_cast<std::size_t>(f.width) * f.height;
+  // Device frames are packed; 16-byte multiples keep every format aligned.
+  const std::size_t din_pitch = (in_bytes + 15) & ~std::size_t{15};
+  const std::size_t dout_pitch = (out_bytes + 15) & ~std::size_t{15};
+  if (int rc = Reserve(&host_in_, din_pitch * frames, "frame staging")) return rc;
+  if (int rc = Reserve(&host_rgba_, dout_pitch * frames, "frame output staging")) return rc;
+  if (f.indices && Reserve(&host_idx_, npx * frames, "index staging")) return RDB_E_NOMEM;
+  cudaStream_t s = stream_;
+  cudaSetDevice(device_);
+  cudaError_t e;
+  if (in_pitch == din_pitch) {
+    e = cudaMemcpyAsync(host_in_.ptr, f.in, in_pitch * frames, cudaMemcpyHostToDevice, s);
+  } else {
+    e = cudaMemcpy2DAsync(host_in_.ptr, din_pitch, f.in, in_pitch, in_bytes, frames,
+                          cudaMemcpyHostToDevice, s);
+  }
+  if (e != cudaSuccess) return CudaFail(e, "frame upload");
+  if (f.indices) cudaMemsetAsync(host_idx_.ptr, 0, npx * frames, s);
+  rdb_frames d = f;
+  d.in = host_in_.ptr;
+  d.in_frame_bytes = din_pitch;
+  d.out = (f.out_format == RDB_RGBAF32 && f.in_format == RDB_RGBAF32 && f.out == f.in)
+              ? host_in_.ptr
+              : host_rgba_.ptr;
+  d.out_frame_bytes = dout_pitch;
+  d.indices = f.indices ? static_cast<uint8_t*>(host_idx_.ptr) : nullptr;
+  if (int rc = Frames(d, o, s)) return rc;
+  if (out_pitch == dout_pitch) {
+    e = cudaMemcpyAsync(f.out, d.out, out_pitch * frames, cudaMemcpyDeviceToHost, s);
+  } else {
+    e = cudaMemcpy2DAsync(f.out, out_pitch, d.out, dout_pitch, out_bytes, frames,
+                          cudaMemcpyDeviceToHost, s);
+  }
+  if (e != cudaSuccess) return CudaFail(e, "frame download");
+  if (f.indices) {
+    e = cudaMemcpyAsync(f.indices, d.indices, npx * frames, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return CudaFail(e, "index download");
+  }
+  return Synchronize(s);
 }
 
 int Context::Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {

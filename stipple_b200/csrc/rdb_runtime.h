@@ -21,6 +21,8 @@ namespace rdb {
 void SetError(const std::string& msg);
 const char* LastError();
 std::size_t BytesPerPixel(int layout);
+// Bytes of one packed frame of an RDB_* format, 0 when unknown or invalid.
+std::size_t FrameBytes(int format, int width, int height);
 int Fail(int code, const std::string& msg);
 int CudaFail(cudaError_t e, const char* what);
 std::string CudaErr(cudaError_t e, const char* what);
@@ -68,6 +70,9 @@ class Context {
 
   int Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_options& o);
+  // Video frames through the blocks engine (rdb_dither_frames).
+  int Frames(const rdb_frames& f, const rdb_options& o, cudaStream_t s);
+  int FramesHost(const rdb_frames& f, const rdb_options& o);
   int Synchronize(cudaStream_t s);
 
   std::size_t bytes() const { return bytes_; }
@@ -84,6 +89,9 @@ class Context {
   int SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  int RunBlocks(int pid, int layout, std::vector<BlockImage>& imgs, const rdb_options& o,
+                cudaStream_t s);
+  int CheckFrames(const rdb_frames& f) const;
   int Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int CheckJob(const rdb_job& j) const;
   void Release(DevBuf* b);

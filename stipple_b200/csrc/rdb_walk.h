@@ -47,18 +47,24 @@ cudaError_t LaunchSeqWalk(const SeqLaunch& L, int grid, cudaStream_t stream);
 // memo (src/rd_riemersma_cpu.cpp:632-697).
 struct BlockImage {
   const unsigned char* pixels;
-  int64_t row_stride;
+  int64_t row_stride;           // bytes (packed frames: width * bytes per pixel)
   int width;
   int height;
-  int layout;
+  int layout;                   // any RDB_* input format (rdb.h)
   int n;                        // block-list length (BlockListLength)
   const int32_t* order;         // sequential order of the geometry (W*H entries)
-  uint8_t* indices;             // palette index per pixel, row-major
+  uint8_t* indices;             // optional palette index per pixel, row-major
   float4* rgba_out;             // optional RgbaF result
   int64_t first_block;          // prefix over images
   int nblocks;
-  int pad;
+  int out_format;               // raw_out's format: RDB_RGBA16 or RDB_YUV444P8
+  unsigned char* raw_out;       // optional encoder-format result
 };
+
+// Writes every pixel's source value into the image's outputs (RgbaF and/or
+// raw) -- the result the block engine leaves where it visits nothing (a 1x1
+// image).
+cudaError_t LaunchSourceFill(const BlockImage& im, cudaStream_t stream);
 
 struct BlockLaunch {
   const BlockImage* images;
@@ -71,7 +77,8 @@ struct BlockLaunch {
   const unsigned char* plan;    // one palette for the launch
   int plan_smem;
   int assoc;                    // the palette associates alpha
-  int is_float;                 // RgbaF input (cx holds float4 per position)
+  int is_float;                 // cx holds the sample widened to float4 (every layout but
+                                // RGB8 / RGBA8, which pack into one word)
   int pad;
   double sw[16];
   int* status;

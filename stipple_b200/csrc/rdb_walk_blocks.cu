@@ -17,15 +17,110 @@
 //            names rotate instead of moving data; the palette plan is staged
 //            in shared memory
 //   scatter  index per pixel through the order table, skipping position 0
+//
+// Video frames add the decoder's and encoder's byte formats on either side
+// (src/rd_riemersma_cpu.cpp:489-516 gather, :711-753 scatter): the gather
+// widens 16-bit or YCbCr input to the Q16 float a reader would have produced,
+// and the scatter narrows the palette colour straight to rgba64 or planar
+// YCbCr, so no RgbaF frame is ever stored.
 #include <cuda_runtime.h>
 
 #include "rdb_curve.h"
 #include "rdb_device.cuh"
 #include "rdb_walk.h"
 #include "rdb_walk_thread.cuh"
+#include "../../include/rdb.h"
 
 namespace rdb {
 namespace {
+
+// swscale's fixed-point BT.601 limited-range YCbCr -> 16-bit RGB, the
+// reference's SwsYuvToRgb16 (include/rd_types.h:75-97): luma (y - 16) scaled
+// by 9539 * 512, chroma (c - 128) * 512 by the v2r / v2g / u2g / u2b
+// coefficients 13075, -6660, -3209 and 16525, all in 32-bit integers (no
+// intermediate exceeds 2^31 for 8-bit inputs), shifted down by 14 and
+// clamped around the 2^15 offset.
+__device__ __forceinline__ float sws_clip16(int acc) {
+  const int v = (acc >> 14) + 32768;
+  return static_cast<float>(v < 0 ? 0 : (v > 65535 ? 65535 : v));
+}
+__device__ __forceinline__ float4 ycbcr_to_q16(unsigned y, unsigned cb, unsigned cr) {
+  const int luma = (static_cast<int>(y) - 16) * (9539 * 512) + (1 << 13) - (1 << 29);
+  const int u = (static_cast<int>(cb) - 128) * 512;
+  const int v = (static_cast<int>(cr) - 128) * 512;
+  return make_float4(sws_clip16(luma + v * 13075), sws_clip16(luma - v * 6660 - u * 3209),
+                     sws_clip16(luma + u * 16525), 65535.0f);
+}
+
+// 4:2:0 chroma at full-resolution pixel (x, y): the 2x bilinear
+// reconstruction of the reference's 4:2:0 gather (src/rd_blocks_cuda.cu:
+// 660-676): weights (2 - ox, ox) x (2 - oy, oy) over the sample at (x/2, y/2)
+// and its right / lower neighbours (edge-replicated), rounded, over 4.
+__device__ __forceinline__ unsigned chroma420(const unsigned char* plane, int w2, int h2, int x,
+                                              int y) {
+  const int cx = x >> 1, cy = y >> 1, ox = x & 1, oy = y & 1;
+  const int cx1 = cx + 1 < w2 ? cx + 1 : cx;
+  const int cy1 = cy + 1 < h2 ? cy + 1 : cy;
+  const unsigned char* r0 = plane + static_cast<int64_t>(cy) * w2;
+  const unsigned char* r1 = plane + static_cast<int64_t>(cy1) * w2;
+  const int top = r0[cx] * (2 - ox) + r0[cx1] * ox;
+  const int bot = r1[cx] * (2 - ox) + r1[cx1] * ox;
+  return static_cast<unsigned>((top * (2 - oy) + bot * oy + 2) >> 2);
+}
+
+// The source value of pixel `pix` as the reader's RgbaF, for every input
+// format (src/rd_riemersma_cpu.cpp:496-516: a uint16 widens exactly; absent
+// alpha reads 65535).
+__device__ __forceinline__ float4 load_wide(const BlockImage& im, int pix) {
+  switch (im.layout) {
+    case RDB_RGB16: {
+      const uint16_t* q = reinterpret_cast<const uint16_t*>(im.pixels) + 3 * static_cast<int64_t>(pix);
+      return make_float4(q[0], q[1], q[2], 65535.0f);
+    }
+    case RDB_RGBA16: {
+      const ushort4 q = reinterpret_cast<const ushort4*>(im.pixels)[pix];
+      return make_float4(q.x, q.y, q.z, q.w);
+    }
+    case RDB_YUV444P8: {
+      const int64_t plane = static_cast<int64_t>(im.width) * im.height;
+      return ycbcr_to_q16(im.pixels[pix], im.pixels[plane + pix], im.pixels[2 * plane + pix]);
+    }
+    case RDB_YUV420P8: {
+      const int64_t plane = static_cast<int64_t>(im.width) * im.height;
+      const int w2 = im.width >> 1, h2 = im.height >> 1;
+      const int y = pix / im.width, x = pix - y * im.width;
+      const unsigned char* cb = im.pixels + plane;
+      const unsigned char* cr = cb + static_cast<int64_t>(w2) * h2;
+      return ycbcr_to_q16(im.pixels[pix], chroma420(cb, w2, h2, x, y), chroma420(cr, w2, h2, x, y));
+    }
+    default:
+      return load_sample(im.pixels, im.layout, im.row_stride, im.width, pix);
+  }
+}
+
+// The encoder-format store of one pixel whose Q16 colour is (r, g, b, a):
+// rgba64 takes the uint16 of each float (src/rd_riemersma_cpu.cpp:746-752);
+// planar YCbCr takes BT.601 limited range of each channel's top 8 bits
+// (:719-731).
+__device__ __forceinline__ void store_raw(const BlockImage& im, int pix, float r, float g, float b,
+                                          float a) {
+  if (im.out_format == RDB_RGBA16) {
+    reinterpret_cast<ushort4*>(im.raw_out)[pix] =
+        make_ushort4(static_cast<uint16_t>(r), static_cast<uint16_t>(g), static_cast<uint16_t>(b),
+                     static_cast<uint16_t>(a));
+    return;
+  }
+  const int r8 = static_cast<int>(r) >> 8;
+  const int g8 = static_cast<int>(g) >> 8;
+  const int b8 = static_cast<int>(b) >> 8;
+  const int y = ((66 * r8 + 129 * g8 + 25 * b8 + 128) >> 8) + 16;
+  const int u = ((-38 * r8 - 74 * g8 + 112 * b8 + 128) >> 8) + 128;
+  const int v = ((112 * r8 - 94 * g8 - 18 * b8 + 128) >> 8) + 128;
+  const int64_t plane = static_cast<int64_t>(im.width) * im.height;
+  im.raw_out[pix] = static_cast<unsigned char>(min(max(y, 0), 255));
+  im.raw_out[plane + pix] = static_cast<unsigned char>(min(max(u, 0), 255));
+  im.raw_out[2 * plane + pix] = static_cast<unsigned char>(min(max(v, 0), 255));
+}
 
 struct V4 {
   double r, g, b, a;
@@ -69,9 +164,8 @@ __global__ void BlockGather(BlockLaunch L, int64_t total) {
     atomicExch(L.status, kDevBadItem);
     pix = 0;
   }
-  if (im.layout == 16) {
-    const float4 s = load_sample(im.pixels, 16, im.row_stride, im.width, pix);
-    reinterpret_cast<float4*>(L.cx)[i] = s;
+  if (L.is_float) {
+    reinterpret_cast<float4*>(L.cx)[i] = load_wide(im, pix);
   } else {
     L.cx[i] = pack_sample(im.pixels, im.layout, im.row_stride, im.width, pix);
   }
@@ -255,24 +349,39 @@ __global__ void BlockScatter(BlockLaunch L, int64_t total) {
   const int64_t npix = static_cast<int64_t>(im.width) * im.height;
   if (pos == 0 && im.n > 1) {
     // This thread also fills the unvisited cell (2^L-1, 0) when it is inside
-    // the image, i.e. when the list is one shorter than pixels + 1.
-    if (im.n == npix && im.rgba_out) {
+    // the image, i.e. when the list is one shorter than pixels + 1: the
+    // source value, in every output asked for (src/rd_riemersma_cpu.cpp:
+    // 776-801 for the encoder formats).
+    if (im.n == npix && (im.rgba_out || im.raw_out)) {
       const int gap = im.width - 1;
-      im.rgba_out[gap] = load_sample(im.pixels, im.layout, im.row_stride, im.width, gap);
+      const float4 src = load_wide(im, gap);
+      if (im.rgba_out) im.rgba_out[gap] = src;
+      if (im.raw_out) store_raw(im, gap, src.x, src.y, src.z, src.w);
     }
     return;
   }
   int pix = (pos == im.n - 1) ? 0 : im.order[pos];
   if (static_cast<unsigned>(pix) >= static_cast<unsigned>(im.width * im.height)) return;
   const uint8_t index = L.chosen[i];
-  im.indices[pix] = index;
-  if (im.rgba_out) {
+  if (im.indices) im.indices[pix] = index;
+  if (im.rgba_out || im.raw_out) {
+    // The colour as clamp_to_quantum's floats; alpha from the palette when it
+    // associates alpha, else the source's, which the scatter leaves in place.
     const PlanHeader* h = reinterpret_cast<const PlanHeader*>(L.plan);
     const float4 pc = reinterpret_cast<const float4*>(L.plan + h->off_out)[index];
-    const float a = h->assoc ? pc.w
-                             : load_sample(im.pixels, im.layout, im.row_stride, im.width, pix).w;
-    im.rgba_out[pix] = make_float4(pc.x, pc.y, pc.z, a);
+    const float a = h->assoc ? pc.w : load_wide(im, pix).w;
+    if (im.rgba_out) im.rgba_out[pix] = make_float4(pc.x, pc.y, pc.z, a);
+    if (im.raw_out) store_raw(im, pix, pc.x, pc.y, pc.z, a);
   }
+}
+
+__global__ void SourceFill(BlockImage im) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<int64_t>(im.width) * im.height) return;
+  const int pix = static_cast<int>(i);
+  const float4 src = load_wide(im, pix);
+  if (im.rgba_out) im.rgba_out[pix] = src;
+  if (im.raw_out) store_raw(im, pix, src.x, src.y, src.z, src.w);
 }
 
 __global__ void CopySource(const unsigned char* pixels, int64_t stride, int width, int height,
@@ -293,12 +402,17 @@ cudaError_t LaunchCopySource(const unsigned char* pixels, int64_t stride, int wi
   return cudaGetLastError();
 }
 
+cudaError_t LaunchSourceFill(const BlockImage& im, cudaStream_t stream) {
+  const int64_t n = static_cast<int64_t>(im.width) * im.height;
+  if (n <= 0 || (!im.rgba_out && !im.raw_out)) return cudaSuccess;
+  SourceFill<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(im);
+  return cudaGetLastError();
+}
+
 cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
   if (total_positions <= 0 || L.total_blocks <= 0) return cudaSuccess;
   const unsigned g1 = static_cast<unsigned>((total_positions + 255) / 256);
   BlockGather<<<g1, 256, 0, stream>>>(L, total_positions);
-  const PlanHeader* hp = nullptr;
-  (void)hp;
   cudaError_t e = L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, stream) : LaunchWalk<true, false>(L, stream))
                           : (L.is_float ? LaunchWalk<false, true>(L, stream) : LaunchWalk<false, false>(L, stream));
   if (e != cudaSuccess) return e;

@@ -219,11 +219,10 @@ std::string RiemersmaBlocksCuda(const Palette& palette, const DitherParams& para
   if (palette.count > 256) return "riemersma-b200: the block engine takes at most 256 colours";
   if (options.block < 16) return "riemersma-b200: block must be >= 16";
   if (state_slot < 0 || state_slot >= kGpuStateSlots) return "riemersma-b200: bad state slot";
-  // Fused 16-bit / YUV feeds and outputs are not part of this engine yet.
-  if (out_u16 || in_u16 || options.emit_u16 || options.emit_yuv444 || options.upload_u16 ||
-      options.in_mode != BlockOptions::InMode::Interleaved16) {
-    return "riemersma-b200: only the RgbaF in-place form of the block engine is implemented";
-  }
+  // The fused forms are selected as the reference selects them
+  // (src/rd_blocks_cuda.cu:1063-1071): a flag AND its buffer.
+  const bool fused_out = options.emit_u16 && out_u16 != nullptr;
+  const bool fused_in = options.upload_u16 && in_u16 != nullptr;
   Slot& s = g_slots[state_slot];
   std::lock_guard<std::mutex> lock(s.mu);
   int pid = 0;
@@ -233,9 +232,55 @@ std::string RiemersmaBlocksCuda(const Palette& palette, const DitherParams& para
   rdb_options_default(&o);
   o.diffusion = params.diffusion;
   o.block = options.block;
-  err = DitherFrames(s, RDB_ENGINE_BLOCKS, pid, width, height, batch, options.frames, o);
-  if (err.empty()) DeviceName(device_name);
-  return err;
+  if (!fused_out && !fused_in) {
+    err = DitherFrames(s, RDB_ENGINE_BLOCKS, pid, width, height, batch, options.frames, o);
+    if (err.empty()) DeviceName(device_name);
+    return err;
+  }
+  if (width == 0 || height == 0) return "riemersma-b200: empty image";
+  if (width > 0x7FFFFFFF || height > 0x7FFFFFFF) return "riemersma-b200: image too large";
+  if (options.frames < 1) return "riemersma-b200: frames must be >= 1";
+  rdb_frames f{};
+  f.width = static_cast<int>(width);
+  f.height = static_cast<int>(height);
+  f.frames = options.frames;
+  f.palette_id = pid;
+  if (fused_in) {
+    // `in_u16` holds the decoder's bytes: uint16 samples, or planar 8-bit
+    // YCbCr (the pointer type is the reference's, not the data's).  The
+    // prepass variant converts the same planes through a uint16 RGB frame,
+    // which is the same widening.
+    switch (options.in_mode) {
+      case BlockOptions::InMode::Interleaved16:
+        f.in_format = options.in_channels == 3 ? RDB_RGB16 : RDB_RGBA16;
+        break;
+      case BlockOptions::InMode::PlanarYuv444:
+      case BlockOptions::InMode::PlanarYuv444Prepass:
+        f.in_format = RDB_YUV444P8;
+        break;
+      case BlockOptions::InMode::PlanarYuv420:
+        f.in_format = RDB_YUV420P8;
+        break;
+      default:
+        return "riemersma-b200: unknown input mode";
+    }
+    f.in = in_u16;
+  } else {
+    if (!batch) return "riemersma-b200: no pixels";
+    f.in = batch;
+    f.in_format = RDB_RGBAF32;
+  }
+  if (fused_out) {
+    f.out = out_u16;
+    f.out_format = options.emit_yuv444 ? RDB_YUV444P8 : RDB_RGBA16;
+  } else {
+    if (!batch) return "riemersma-b200: no output buffer";
+    f.out = batch;
+    f.out_format = RDB_RGBAF32;
+  }
+  if (rdb_dither_frames_host(s.ctx, &f, &o) != RDB_OK) return Err("dither");
+  DeviceName(device_name);
+  return {};
 }
 
 std::string RiemersmaApproxCuda(const Palette& palette, const DitherParams& params,

@@ -94,3 +94,39 @@ def log_uniform_sizes(n: int, seed: int, lo: int = 1, hi: int = 4096):
     ws = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(int)
     hs = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(int)
     return [(int(max(lo, w)), int(max(lo, h))) for w, h in zip(ws, hs)]
+
+
+# ---- decoder-format video frames --------------------------------------------
+# Synthetic stand-ins for what a video decoder hands the block engine: the same
+# gradient frames, widened to 16 bits with seeded low-order detail, or
+# converted to planar 8-bit YCbCr (BT.601 limited range, rounded; 4:2:0 takes
+# the rounded mean of each 2x2 chroma quad).
+
+def rgb16_frame(img8: np.ndarray, seed: int) -> np.ndarray:
+    """uint8 (H, W, C) -> uint16 (H, W, C): v * 257 plus seeded noise in
+    [-96, 96], clipped; an alpha channel keeps its exact v * 257."""
+    rng = np.random.default_rng(seed ^ 0x16161616)
+    v = img8.astype(np.int32) * 257
+    noise = rng.integers(-96, 97, v.shape, dtype=np.int32)
+    if img8.shape[2] == 4:
+        noise[:, :, 3] = 0
+    return np.clip(v + noise, 0, 65535).astype(np.uint16)
+
+
+def yuv444_frame(img8: np.ndarray) -> np.ndarray:
+    """uint8 (H, W, >=3) RGB -> planar Y, Cb, Cr (3, H, W) uint8."""
+    rgb = img8[:, :, :3].astype(np.float64)
+    r, g, b = rgb[:, :, 0], rgb[:, :, 1], rgb[:, :, 2]
+    y = 16 + (65.481 * r + 128.553 * g + 24.966 * b) / 255.0
+    cb = 128 + (-37.797 * r - 74.203 * g + 112.0 * b) / 255.0
+    cr = 128 + (112.0 * r - 93.786 * g - 18.214 * b) / 255.0
+    return np.clip(np.rint(np.stack([y, cb, cr])), 0, 255).astype(np.uint8)
+
+
+def yuv420_frame(img8: np.ndarray) -> np.ndarray:
+    """uint8 (H, W, >=3) RGB, H and W even -> the packed 4:2:0 frame bytes:
+    Y (H*W) then Cb and Cr (H/2 * W/2 each)."""
+    p = yuv444_frame(img8).astype(np.int32)
+    h, w = p.shape[1:]
+    c = (p[1:, 0::2, 0::2] + p[1:, 0::2, 1::2] + p[1:, 1::2, 0::2] + p[1:, 1::2, 1::2] + 2) >> 2
+    return np.concatenate([p[0].reshape(-1), c[0].reshape(-1), c[1].reshape(-1)]).astype(np.uint8)

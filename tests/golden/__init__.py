@@ -13,7 +13,7 @@ def cases():
     """Yields (name, rgbaf float32 HxWx4, list of per-case dicts)."""
     for path in sorted(glob.glob(os.path.join(HERE, "*.npz"))):
         name = os.path.basename(path)[:-4]
-        if name == "curves":
+        if name in ("curves", "frames"):
             continue
         z = np.load(path)
         if "rgba8" in z:
@@ -29,3 +29,11 @@ def cases():
 
 def curves():
     return np.load(os.path.join(HERE, "curves.npz"))
+
+
+def frames():
+    """Yields the fused-format block-walk cases of frames.npz as dicts."""
+    z = np.load(os.path.join(HERE, "frames.npz"))
+    for i in range(int(z["ncases"])):
+        pre = f"c{i}_"
+        yield {k[len(pre):]: z[k] for k in z.files if k.startswith(pre)}

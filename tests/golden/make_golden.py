@@ -6,13 +6,15 @@ and src/rd_riemersma_cpu.cpp compiled unmodified by oracle/Makefile) on
 * the reference's PNG test fixtures (tests/*.png of the reference tree,
   decoded with PIL the way an 8-bit decode into Q16 is scaled: v * 257, and
   16-bit samples as-is), and
-* seeded synthetic images of the benchmark configurations,
+* seeded synthetic images of the benchmark configurations, and
+* seeded decoder-format video frames (rgb48 / rgba64 / planar 4:4:4 / RgbaF)
+  through the block walk's fused gather and output (frames.npz),
 
 and stores inputs and outputs as compressed .npz files.  The GPU tests and the
 oracle tests compare against these files; the reference tree is not needed at
 test time.  Re-run with:
 
-    make -f oracle/Makefile && python tests/golden/make_golden.py [REF_DIR]
+    make -f oracle/Makefile && python tests/golden/make_golden.py [REF_DIR] [--frames-only]
 """
 from __future__ import annotations
 
@@ -110,8 +112,71 @@ def save(name: str, rgbaf: np.ndarray, recs: list[dict]) -> None:
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
 
 
+def frames_golden(ref: RefLib) -> None:
+    """RiemersmaBlocksCpu with gather_raw / raw_out on small seeded frames.
+    Each case k stores: in (F, bytes) uint8, gather layout / channels (0 =
+    RgbaF input), tree_src RgbaF, w, h, colors, assoc, block, and out_yuv /
+    out_rgba64 (F, bytes) uint8."""
+    arrays = {}
+    cases = [  # (w, h, input, channels, alpha, assoc, colors, block)
+        (32, 24, "u16", 4, True, False, 16, 32),
+        (32, 24, "u16", 4, True, True, 64, 16),
+        (37, 29, "u16", 3, False, False, 32, 16),
+        (32, 24, "yuv", 0, False, False, 256, 64),
+        (37, 29, "yuv", 0, False, False, 8, 512),
+        (32, 24, "f32", 4, True, False, 16, 32),
+        (1, 1, "u16", 4, True, False, 4, 16),
+    ]
+    for k, (w, h, kind, ch, alpha, assoc, colors, block) in enumerate(cases):
+        fr8 = [synth.video_frame(w, h, 600 + k, f) for f in range(2)]
+        if alpha:
+            a = synth.alpha_mask(w, h, 600 + k)
+            fr8 = [np.concatenate([f, a[:, :, None]], axis=2) for f in fr8]
+        if kind == "u16":
+            fr = [synth.rgb16_frame(f[:, :, :ch], 700 + k + i) for i, f in enumerate(fr8)]
+            raw = np.stack([f.reshape(-1).view(np.uint8) for f in fr])
+            layout = 4
+            tree_src = np.zeros((h, w, 4), np.float32)
+            tree_src[:, :, :ch] = fr[0].astype(np.float32)
+            if ch == 3:
+                tree_src[:, :, 3] = 65535.0
+        elif kind == "yuv":
+            fr = [synth.yuv444_frame(f) for f in fr8]
+            raw = np.stack([f.reshape(-1) for f in fr])
+            layout, ch = 3, 0
+            tree_src = None  # widened by the reference-side gather of frame 0 below
+        else:
+            fr = [synth.to_q16(f) for f in fr8]
+            raw = np.stack([f.reshape(-1).view(np.uint8) for f in fr])
+            layout, ch = 0, 0
+            tree_src = fr[0]
+        if tree_src is None:
+            # The palette's source image only: frame 0 widened by the oracle,
+            # since the reference exposes no widening entry point.  Every
+            # stored output is the reference's own.
+            from pyoracle import Oracle
+            tree_src = Oracle().widen_frame(444, raw[0], w, h)
+        src = np.stack(fr).astype(np.float32) if layout == 0 else raw
+        outs = {}
+        for yuv in (True, False):
+            rc, msg, out = ref.walk_blocks_raw(tree_src, src, layout, ch, w, h, yuv, colors,
+                                               assoc, block)
+            assert rc == 0, msg
+            outs["out_yuv" if yuv else "out_rgba64"] = out
+        rec = dict(inp=raw, layout=layout, channels=ch, tree_src=tree_src, w=w, h=h,
+                   colors=colors, assoc=int(assoc), block=block, **outs)
+        for key, v in rec.items():
+            arrays[f"c{k}_{key}"] = np.asarray(v)
+    arrays["ncases"] = np.asarray(len(cases))
+    np.savez_compressed(os.path.join(HERE, "frames.npz"), **arrays)
+    print("frames", len(cases))
+
+
 def main(ref_dir: str) -> None:
     ref = RefLib()
+    frames_golden(ref)
+    if "--frames-only" in sys.argv:
+        return
     # The reference's own fixtures.
     for fx in FIXTURES:
         rgbaf, alpha = decode(os.path.join(ref_dir, "tests", fx + ".png"))
@@ -143,4 +208,5 @@ def main(ref_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else "/root/reference")
