@@ -165,9 +165,16 @@ def test_frames_refusals(ctx, oracle):
     raw, _ = _decoder_frames(sb.YUV444P8, _frames8(w, h, 1, 1, False), 0)
     pid = _palette(ctx, oracle.widen_frame(sb.YUV444P8, raw[0], w, h), 16, False)
     try:
+        import torch
+        # Room for either frame at either offset: the host refuses these
+        # before anything is enqueued.
+        buf = torch.zeros(16384, dtype=torch.uint8, device="cuda")
         with pytest.raises(sb.RdbError, match="even width and height"):
-            ctx.dither_frames_host(np.zeros(w * h * 2, np.uint8), sb.YUV420P8, w, h, pid,
-                                   sb.YUV444P8)
+            ctx.dither_frames(buf.data_ptr(), sb.YUV420P8, w, h, 1, pid, buf.data_ptr() + 8192,
+                              sb.YUV444P8)
+        with pytest.raises(sb.RdbError, match="in place"):
+            ctx.dither_frames(buf.data_ptr(), sb.YUV444P8, w, h, 1, pid, buf.data_ptr(),
+                              sb.YUV444P8)
         with pytest.raises(sb.RdbError, match="output frame format"):
             ctx.dither_frames_host(raw, sb.YUV444P8, w, h, pid, sb.RGB8)
         with pytest.raises(sb.RdbError, match="at least 16"):
