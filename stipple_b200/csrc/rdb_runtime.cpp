@@ -1167,10 +1167,13 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       }
       tune->ms.assign(tune->cand.size(), -1.0);
     }
-    for (std::size_t c = 0; c < tune->cand.size() && tune_slot < 0; ++c) {
+    for (std::size_t c = 0; c < tune->cand.size() && tune_slot < 0 && tune->warmed; ++c) {
       if (tune->ms[c] == -1.0) tune_slot = static_cast<int>(c);
     }
-    if (tune_slot >= 0) {
+    if (!tune->warmed) {
+      tune->warmed = true;
+      seg_len = tune->cand[0];
+    } else if (tune_slot >= 0) {
       tune->ms[static_cast<std::size_t>(tune_slot)] = -2.0;
       seg_len = tune->cand[static_cast<std::size_t>(tune_slot)];
     } else {
@@ -1321,28 +1324,10 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   }
   if ((e = LaunchTswGather(L, positions, s)) != cudaSuccess) return CudaFail(e, "sample gather");
 
-  // The tuner times the passes on the device (setup and uploads excluded).
-  const bool timing = tune && tune_slot >= 0;
-  if (timing) {
-    for (cudaEvent_t& ev : tune_ev_) {
-      if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return CudaFail(e, "tuner events");
-    }
-    cudaEventRecord(tune_ev_[0], s);
-  }
   const int max_passes_opt = o.max_passes > 0 ? o.max_passes : 1 << 30;
   const bool device_loop = o.loop_mode == 2 || (o.loop_mode == 0 && !profiling_);
   if (o.loop_mode < 0 || o.loop_mode > 2) return Fail(RDB_E_INVALID, "loop_mode must be 0..2");
   if (device_loop) {
-    // Passes 0 and 1 from the host (pass 0 is the warm-up pass), then the
-    // rest as one graph launch: nothing here waits for the device.
-    for (int pass = 0; pass < 2; ++pass) {
-      L.pass = pass;
-      L.tag = static_cast<uint32_t>(pass + 1);
-      cudaMemsetAsync(L.bad[pass & 1], 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
-      if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
-      if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
-      if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
-    }
     if (int rc = Reserve(&tsw_ctl_, 64, "loop control")) return rc;
     static const int kCtlInit[8] = {0, 0, 0, 0, 3, 0, 0, 0};  // counters, then the tag of pass 2
     int* ctl = static_cast<int*>(tsw_ctl_.ptr);
@@ -1376,6 +1361,27 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
         return CudaFail(e, "pass-loop graph instantiation");
       }
       loop_key_ = key;
+    }
+  }
+  // The tuner times the passes on the device: setup, uploads and the graph's
+  // instantiation above are outside its events.
+  const bool timing = tune && tune_slot >= 0;
+  if (timing) {
+    for (cudaEvent_t& ev : tune_ev_) {
+      if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return CudaFail(e, "tuner events");
+    }
+    cudaEventRecord(tune_ev_[0], s);
+  }
+  if (device_loop) {
+    // Passes 0 and 1 from the host (pass 0 is the warm-up pass), then the
+    // rest as one graph launch: nothing here waits for the device.
+    for (int pass = 0; pass < 2; ++pass) {
+      L.pass = pass;
+      L.tag = static_cast<uint32_t>(pass + 1);
+      cudaMemsetAsync(L.bad[pass & 1], 0x7F, static_cast<std::size_t>(n) * sizeof(int), s);
+      if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
+      if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
+      if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
     }
     if ((e = cudaGraphLaunch(loop_exec_, s)) != cudaSuccess) return CudaFail(e, "pass-loop graph launch");
     if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");

@@ -52,6 +52,10 @@ struct DevPlan {
 struct SegTune {
   std::vector<int> cand;
   std::vector<double> ms;  // -1 = not yet measured, -2 = being measured
+  // The first call of a workload runs untimed: it pays one-time costs (module
+  // loading on first launch, uniform tables) that would bias whichever
+  // candidate came first.
+  bool warmed = false;
 };
 
 class Context {
