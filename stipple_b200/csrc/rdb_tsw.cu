@@ -97,6 +97,32 @@ __device__ __forceinline__ void sample(const TswLaunch& L, int64_t at, double (&
   }
 }
 
+// Pixel t (slot U) takes its last term w15 * e_{t-1}: the head of a step,
+// the only part its colour lookup waits for.
+template <int U, int C>
+__device__ __forceinline__ void RotateHead(const double (&sw)[16], const double (&R)[16][C],
+                                           const double (&e)[C], double (&v)[C]) {
+#pragma unroll
+  for (int c = 0; c < C; ++c) v[c] = __dadd_rn(R[U][c], __dmul_rn(sw[15], e[c]));
+}
+
+// The rest of the step's rotation: the 15 pixels after pixel t take e_{t-1}
+// with their weights and slot U is refilled with pixel t + 16.  Issued after
+// the lookup's loads, so their latency overlaps this arithmetic.
+template <int U, int C>
+__device__ __forceinline__ void RotateTail(const double (&sw)[16], double (&R)[16][C],
+                                           const double (&e)[C], const double (&p)[C]) {
+#pragma unroll
+  for (int jj = 1; jj < 16; ++jj) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      R[(U + jj) & 15][c] = __dadd_rn(R[(U + jj) & 15][c], __dmul_rn(sw[15 - jj], e[c]));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < C; ++c) R[U][c] = p[c];
+}
+
 // Pixel t (slot U) takes its last term w15 * e_{t-1}; the 15 pixels after it
 // take e_{t-1} with their weights; slot U is refilled with pixel t + 16.
 template <int U, int C>
@@ -257,32 +283,35 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
       if (t + 16 < end) sample<kFloat, C>(L, base + t + 16, p);
       double v[C];
       switch (u) {
-        case 0: Rotate<0, C>(L.sw, R, e, v, p); break;
-        case 1: Rotate<1, C>(L.sw, R, e, v, p); break;
-        case 2: Rotate<2, C>(L.sw, R, e, v, p); break;
-        case 3: Rotate<3, C>(L.sw, R, e, v, p); break;
-        case 4: Rotate<4, C>(L.sw, R, e, v, p); break;
-        case 5: Rotate<5, C>(L.sw, R, e, v, p); break;
-        case 6: Rotate<6, C>(L.sw, R, e, v, p); break;
-        case 7: Rotate<7, C>(L.sw, R, e, v, p); break;
-        case 8: Rotate<8, C>(L.sw, R, e, v, p); break;
-        case 9: Rotate<9, C>(L.sw, R, e, v, p); break;
-        case 10: Rotate<10, C>(L.sw, R, e, v, p); break;
-        case 11: Rotate<11, C>(L.sw, R, e, v, p); break;
-        case 12: Rotate<12, C>(L.sw, R, e, v, p); break;
-        case 13: Rotate<13, C>(L.sw, R, e, v, p); break;
-        case 14: Rotate<14, C>(L.sw, R, e, v, p); break;
-        default: Rotate<15, C>(L.sw, R, e, v, p); break;
+        case 0: RotateHead<0, C>(L.sw, R, e, v); break;
+        case 1: RotateHead<1, C>(L.sw, R, e, v); break;
+        case 2: RotateHead<2, C>(L.sw, R, e, v); break;
+        case 3: RotateHead<3, C>(L.sw, R, e, v); break;
+        case 4: RotateHead<4, C>(L.sw, R, e, v); break;
+        case 5: RotateHead<5, C>(L.sw, R, e, v); break;
+        case 6: RotateHead<6, C>(L.sw, R, e, v); break;
+        case 7: RotateHead<7, C>(L.sw, R, e, v); break;
+        case 8: RotateHead<8, C>(L.sw, R, e, v); break;
+        case 9: RotateHead<9, C>(L.sw, R, e, v); break;
+        case 10: RotateHead<10, C>(L.sw, R, e, v); break;
+        case 11: RotateHead<11, C>(L.sw, R, e, v); break;
+        case 12: RotateHead<12, C>(L.sw, R, e, v); break;
+        case 13: RotateHead<13, C>(L.sw, R, e, v); break;
+        case 14: RotateHead<14, C>(L.sw, R, e, v); break;
+        default: RotateHead<15, C>(L.sw, R, e, v); break;
       }
 #pragma unroll
       for (int c = 0; c < C; ++c) f[c] = clamp_pixel(v[c]);
       br = byte_dev(f[0]);
       bg = byte_dev(f[1]);
       bb = byte_dev(f[2]);
-      key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12);
       if constexpr (kAssoc) {
         ba = byte_dev(f[3]);
-        key |= (ba >> 2) << 18;
+        key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12) | ((ba >> 2) << 18);
+      } else {
+        // The direct 2^18-entry tables (uniform copy, G maps, usemin) are all
+        // indexed in tiled_key order.
+        key = tiled_key(br >> 2, bg >> 2, bb >> 2);
       }
       // A uniform key's search result (and so its memo value) is fixed by the
       // key: no search, no memo, no bookkeeping.
@@ -297,6 +326,24 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
         uv = __ldg(uni + key);
         slot = static_cast<int>(key);
         if (keyed) gv = __ldg(gprev + key);  // both loads in flight together
+      }
+      switch (u) {
+        case 0: RotateTail<0, C>(L.sw, R, e, p); break;
+        case 1: RotateTail<1, C>(L.sw, R, e, p); break;
+        case 2: RotateTail<2, C>(L.sw, R, e, p); break;
+        case 3: RotateTail<3, C>(L.sw, R, e, p); break;
+        case 4: RotateTail<4, C>(L.sw, R, e, p); break;
+        case 5: RotateTail<5, C>(L.sw, R, e, p); break;
+        case 6: RotateTail<6, C>(L.sw, R, e, p); break;
+        case 7: RotateTail<7, C>(L.sw, R, e, p); break;
+        case 8: RotateTail<8, C>(L.sw, R, e, p); break;
+        case 9: RotateTail<9, C>(L.sw, R, e, p); break;
+        case 10: RotateTail<10, C>(L.sw, R, e, p); break;
+        case 11: RotateTail<11, C>(L.sw, R, e, p); break;
+        case 12: RotateTail<12, C>(L.sw, R, e, p); break;
+        case 13: RotateTail<13, C>(L.sw, R, e, p); break;
+        case 14: RotateTail<14, C>(L.sw, R, e, p); break;
+        default: RotateTail<15, C>(L.sw, R, e, p); break;
       }
       search = uv == kNotUniform;
       index = uv;
