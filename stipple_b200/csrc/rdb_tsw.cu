@@ -123,24 +123,6 @@ __device__ __forceinline__ void RotateTail(const double (&sw)[16], double (&R)[1
   for (int c = 0; c < C; ++c) R[U][c] = p[c];
 }
 
-// Pixel t (slot U) takes its last term w15 * e_{t-1}; the 15 pixels after it
-// take e_{t-1} with their weights; slot U is refilled with pixel t + 16.
-template <int U, int C>
-__device__ __forceinline__ void Rotate(const double (&sw)[16], double (&R)[16][C],
-                                       const double (&e)[C], double (&v)[C], const double (&p)[C]) {
-#pragma unroll
-  for (int c = 0; c < C; ++c) v[c] = __dadd_rn(R[U][c], __dmul_rn(sw[15], e[c]));
-#pragma unroll
-  for (int jj = 1; jj < 16; ++jj) {
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-      R[(U + jj) & 15][c] = __dadd_rn(R[(U + jj) & 15][c], __dmul_rn(sw[15 - jj], e[c]));
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < C; ++c) R[U][c] = p[c];
-}
-
 __device__ __forceinline__ unsigned own_hash(unsigned key) { return (key * 0x9E3779B1u) >> 8; }
 
 // Fire-and-forget minimum (no value comes back, so nothing waits on it).
