@@ -62,7 +62,6 @@ Context::~Context() {
   for (auto& p : plans_) {
     cudaFree(p.second.dev);
     cudaFree(p.second.uniform);
-    cudaFree(p.second.uniform_tiled);
   }
   for (auto& b : free_blocks_) cudaFree(b.second);
   for (auto& o : orders_) cudaFree(o.second);
@@ -273,12 +272,11 @@ int Context::DestroyPalette(int id) {
   cudaStreamSynchronize(stream_);
   FreeBlock(it->second.dev, it->second.dev_bytes);
   FreeBlock(it->second.uniform, kUniformKeys);
-  FreeBlock(it->second.uniform_tiled, kUniformKeys);
   plans_.erase(it);
   return RDB_OK;
 }
 
-int Context::Uniform(int id, cudaStream_t s, const uint8_t** out, bool tiled) {
+int Context::Uniform(int id, cudaStream_t s, const uint8_t** out) {
   auto it = plans_.find(id);
   if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
   DevPlan& p = it->second;
@@ -294,17 +292,7 @@ int Context::Uniform(int id, cudaStream_t s, const uint8_t** out, bool tiled) {
       return CudaFail(e, "uniform-key table");
     }
   }
-  if (tiled && !p.uniform_tiled) {
-    int rc = RDB_OK;
-    p.uniform_tiled = static_cast<uint8_t*>(AllocBlock(kUniformKeys, "uniform-key table", &rc));
-    if (!p.uniform_tiled) return rc;
-    cudaError_t e;
-    if ((e = LaunchUniformTiled(p.uniform, p.uniform_tiled, s)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-      return CudaFail(e, "uniform-key table");
-    }
-  }
-  *out = tiled ? p.uniform_tiled : p.uniform;
+  *out = p.uniform;
   return RDB_OK;
 }
 
@@ -1220,7 +1208,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     im.plan = p->dev;
     im.plan_smem = p->smem;
     if (!assoc) {
-      if (int rc = Uniform(j.palette_id, s, &im.uni, true)) return rc;
+      if (int rc = Uniform(j.palette_id, s, &im.uni)) return rc;
     }
     im.first_seg = total;
     im.nsegs = (im.n + seg_len - 1) / seg_len;

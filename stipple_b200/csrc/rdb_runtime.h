@@ -41,7 +41,6 @@ struct DevPlan {
   int count = 0;
   bool assoc = false;
   uint8_t* uniform = nullptr;  // uniform-key table (rdb_uniform.h), built on first use
-  uint8_t* uniform_tiled = nullptr;  // the same in tiled_key order (thread walker)
 };
 
 // Segment-length autotuner of the segmented walk: per (device, log2 of the
@@ -67,9 +66,8 @@ class Context {
   int CreatePalette(const PlanInput& in, int* id);
   int DestroyPalette(int id);
   const DevPlan* Plan(int id) const;
-  // The palette's uniform-key table, built on the stream on first use; with
-  // `tiled`, its copy in tiled_key order.
-  int Uniform(int id, cudaStream_t s, const uint8_t** out, bool tiled = false);
+  // The palette's uniform-key table, built on the stream on first use.
+  int Uniform(int id, cudaStream_t s, const uint8_t** out);
 
   // Visit order of a geometry, built on first use and kept resident.
   int Order(int width, int height, cudaStream_t s, const int32_t** out);

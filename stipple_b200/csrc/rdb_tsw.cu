@@ -287,13 +287,10 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
       br = byte_dev(f[0]);
       bg = byte_dev(f[1]);
       bb = byte_dev(f[2]);
+      key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12);
       if constexpr (kAssoc) {
         ba = byte_dev(f[3]);
-        key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12) | ((ba >> 2) << 18);
-      } else {
-        // The direct 2^18-entry tables (uniform copy, G maps, usemin) are all
-        // indexed in tiled_key order.
-        key = tiled_key(br >> 2, bg >> 2, bb >> 2);
+        key |= (ba >> 2) << 18;
       }
       // A uniform key's search result (and so its memo value) is fixed by the
       // key: no search, no memo, no bookkeeping.

@@ -47,15 +47,15 @@ struct TswImage {
   uint8_t* indices;
   float4* rgba_out;
   const unsigned char* plan; // device plan blob
-  const uint8_t* uni;        // uniform-key table of the palette, tiled_key order (rdb_uniform.h)
+  const uint8_t* uni;        // uniform-key table of the palette (rdb_uniform.h)
   int plan_smem;
   int first_seg;             // global id of segment 0
   int nsegs;
   int64_t cx_offset;         // first position in the gathered sample / index buffers
   uint32_t* g[2];            // first-touch maps; pass p writes g[p & 1]
   uint32_t* usemin;          // earliest segment that took the key from G_prev
-  // Direct maps (no alpha): g and usemin have 2^18 entries indexed by the
-  // key in tiled_key order and hkeys is null.  Hashed maps (alpha keys, 24 bits): hmask + 1 slots,
+  // Direct maps (no alpha): g and usemin have 2^18 entries indexed by key and
+  // hkeys is null.  Hashed maps (alpha keys, 24 bits): hmask + 1 slots,
   // hkeys[slot] = key + 1 (0 = empty), every inserted slot listed in
   // hlist[0 .. *hcount).
   uint32_t* hkeys;

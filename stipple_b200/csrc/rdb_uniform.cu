@@ -84,17 +84,4 @@ cudaError_t LaunchUniformTable(const unsigned char* plan, uint8_t* out, cudaStre
   return cudaGetLastError();
 }
 
-namespace {
-__global__ void UniformTiledKernel(const uint8_t* table, uint8_t* tiled) {
-  const unsigned key = blockIdx.x * blockDim.x + threadIdx.x;
-  if (key >= static_cast<unsigned>(kUniformKeys)) return;
-  tiled[tiled_key(key & 63u, (key >> 6) & 63u, key >> 12)] = table[key];
-}
-}  // namespace
-
-cudaError_t LaunchUniformTiled(const uint8_t* table, uint8_t* tiled, cudaStream_t s) {
-  UniformTiledKernel<<<kUniformKeys / 256, 256, 0, s>>>(table, tiled);
-  return cudaGetLastError();
-}
-
 }  // namespace rdb

@@ -34,16 +34,4 @@ constexpr uint8_t kNotUniform = 0xFF;
 // `plan`: a device plan blob (rdb_plan.h); `out`: kUniformKeys bytes.
 cudaError_t LaunchUniformTable(const unsigned char* plan, uint8_t* out, cudaStream_t s);
 
-// The colour-tiled key order of the thread walker's per-key tables: the low
-// 3 bits of each channel's 6-bit key select an entry inside an 8x8x8 tile of
-// 512 consecutive keys, the high 3 bits the tile.  Nearby colours then share
-// cache lines in every channel, not only in red.  A bijection on 18 bits.
-__host__ __device__ __forceinline__ unsigned tiled_key(unsigned r6, unsigned g6, unsigned b6) {
-  return ((r6 >> 3) << 15) | ((g6 >> 3) << 12) | ((b6 >> 3) << 9) | ((r6 & 7u) << 6) |
-         ((g6 & 7u) << 3) | (b6 & 7u);
-}
-
-// `tiled[tiled_key(r, g, b)] = table[r | g << 6 | b << 12]` for every key.
-cudaError_t LaunchUniformTiled(const uint8_t* table, uint8_t* tiled, cudaStream_t s);
-
 }  // namespace rdb
