@@ -50,7 +50,7 @@ def parse():
                     help="requests in the served-stream sample (the full stream is 10,000)")
     ap.add_argument("--serve-rates", default="30,120,600",
                     help="Poisson arrival rates (requests/s) of the served-stream sample")
-    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "seq_alpha", "blocks", "batched", "jacobi"],
+    ap.add_argument("--profile-case", default="none", choices=["none", "seq", "seq_alpha", "blocks", "batched", "jacobi", "frames"],
                     help="run only that workload's device steps (for ncu captures) and print "
                          "its timing; no JSON contract line")
     ap.add_argument("--seq-mode", type=int, default=0, help="profile cases: sequential form")
@@ -545,6 +545,26 @@ def profile_case(a):
             jobs.append(dict(pixels=d.data_ptr(), width=w, height=h, layout=sb.RGBA8, palette_id=p,
                              indices=o.data_ptr()))
         opts = {}
+    elif a.profile_case == "frames":
+        n = a.block_frames
+        yuv = np.stack([synth.yuv444_frame(synth.video_frame(W, H, 3, f)).reshape(-1)
+                        for f in range(n)])
+        d_in = torch.from_numpy(yuv).cuda()
+        d_out = torch.empty_like(d_in)
+        for _ in range(a.warmup):
+            ctx.dither_frames(d_in.data_ptr(), sb.YUV444P8, W, H, n, pid, d_out.data_ptr(),
+                              sb.YUV444P8, stream=s, block=512)
+        ctx.synchronize(s)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            ctx.dither_frames(d_in.data_ptr(), sb.YUV444P8, W, H, n, pid, d_out.data_ptr(),
+                              sb.YUV444P8, stream=s, block=512)
+        e1.record(stream)
+        ctx.synchronize(s)
+        print(f"frames: {e0.elapsed_time(e1) / max(1, a.steps):.3f} ms per step", flush=True)
+        return
     elif a.profile_case in ("seq", "seq_alpha", "jacobi"):
         lay = sb.RGB8
         if a.profile_case == "seq_alpha":
