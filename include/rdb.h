@@ -74,6 +74,22 @@ void rdb_octree_colormap(const rdb_octree* t, double* out);
 void rdb_octree_nodes(const rdb_octree* t, int32_t* child, int32_t* parent,
                       uint32_t* color_number, uint64_t* number_unique);
 void rdb_octree_free(rdb_octree* t);
+/* Palette files: rdither's --palette-export / --palette-from text form
+ * (.txt or .text paths).  The writer is ImWritePalette's text branch
+ * (src/rd_im.cpp:994-1030): a header, then per colour "index r g b a hex"
+ * tab-separated, Q16 with six decimals.  The reader is ImReadPalette's
+ * (:1175-1350): rows "index r g b [a] [hex]" (alpha read only when the hex
+ * column follows), indices contiguous from 0 (a gap is refused), r, g, b
+ * rounded through float, colours sorted by (r, g, b, a), and the tree built
+ * from that one-row strip with as many colours as rows (no alpha association;
+ * greyscale when every row is grey) -- refused if it merges any.  The tree's
+ * colormap is then the palette; `associate_alpha` receives 1 when some row's
+ * alpha is not opaque (the reference's palette flag).  `expect_colors` > 0
+ * refuses a file with another count.  Other extensions (the PNG form, which
+ * is ImageMagick's PNG8 codec) return RDB_E_UNSUPPORTED. */
+int rdb_palette_write_text(const double* colors /* count x 4 */, int count, const char* path);
+int rdb_palette_read_text(const char* path, int expect_colors, rdb_octree** out,
+                          int* associate_alpha);
 /* 1 when every pixel has r == g == b (the reference's greyscale rule,
  * src/rd_cli.cpp:2452-2456). */
 int rdb_is_grayscale(const void* pixels, int layout, size_t width, size_t height,

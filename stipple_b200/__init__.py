@@ -150,6 +150,9 @@ SIGNATURES = {
     "rdb_octree_nodes": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rdb_octree_free": (None, [C.c_void_p]),
     "rdb_is_grayscale": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t]),
+    "rdb_palette_write_text": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
+    "rdb_palette_read_text": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_int)]),
     "rdb_context_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
     "rdb_context_destroy": (None, [C.c_void_p]),
     "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
@@ -236,9 +239,14 @@ def layout_of(img: np.ndarray) -> int:
 class Octree:
     """Host palette build with ImageMagick octree semantics (rdb_octree_build)."""
 
-    def __init__(self, img: np.ndarray, max_colors: int, associate_alpha: bool | None = None,
-                 grayscale: bool | None = None):
+    def __init__(self, img: np.ndarray | None, max_colors: int = 0,
+                 associate_alpha: bool | None = None, grayscale: bool | None = None):
         lib = load()
+        if img is None:  # filled by a reader (read_palette_text)
+            self.handle = C.c_void_p()
+            self.associate_alpha = False
+            self.grayscale = False
+            return
         img = np.ascontiguousarray(img)
         lay = layout_of(img)
         h, w = img.shape[:2]
@@ -538,6 +546,23 @@ def inverse_filter(taps: int, diffusion: float = 1.0) -> np.ndarray:
     g = np.zeros(taps + 1, np.float64)
     _check(load().rdb_inverse_filter(taps, diffusion, _ptr(g)))
     return g
+
+
+def write_palette_text(colors: np.ndarray, path: str) -> None:
+    """rdither's palette text file (rdb_palette_write_text): `colors` is
+    (count, 4) Q16 r, g, b, a."""
+    c = np.ascontiguousarray(colors, np.float64).reshape(-1, 4)
+    _check(load().rdb_palette_write_text(_ptr(c), c.shape[0], path.encode()))
+
+
+def read_palette_text(path: str, expect_colors: int = 0) -> tuple[Octree, bool]:
+    """Reads a palette text file (rdb_palette_read_text): the tree built from
+    its colours, and whether the file's palette associates alpha."""
+    t = Octree(None)
+    assoc = C.c_int(0)
+    _check(load().rdb_palette_read_text(path.encode(), int(expect_colors), C.byref(t.handle),
+                                        C.byref(assoc)))
+    return t, bool(assoc.value)
 
 
 def frame_bytes(fmt: int, width: int, height: int) -> int:

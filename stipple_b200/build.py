@@ -37,6 +37,7 @@ SOURCES = [
     "rdb_runtime.cpp",
     "rdb_capi.cpp",
     "rdb_serve.cpp",
+    "rdb_palette_file.cpp",
     "rdb_curve.cu",
     "rdb_walk_seq.cu",
     "rdb_walk_blocks.cu",

@@ -143,6 +143,36 @@ void rdb_octree_nodes(const rdb_octree* t, int32_t* child, int32_t* parent,
 
 void rdb_octree_free(rdb_octree* t) { delete t; }
 
+int rdb_palette_write_text(const double* colors, int count, const char* path) {
+  if (!colors || !path) return Guard("rdb_palette_write_text");
+  return rdb::WritePaletteText(colors, count, path);
+}
+
+int rdb_palette_read_text(const char* path, int expect_colors, rdb_octree** out,
+                          int* associate_alpha) {
+  if (!path || !out) return Guard("rdb_palette_read_text");
+  *out = nullptr;
+  std::vector<float> strip;
+  int count = 0;
+  bool assoc = false, gray = false;
+  if (int rc = rdb::ReadPaletteText(path, expect_colors, &strip, &count, &assoc, &gray)) return rc;
+  rdb_octree* t = new (std::nothrow) rdb_octree();
+  if (!t) return rdb::Fail(RDB_E_NOMEM, "octree allocation");
+  t->tree.Build(strip.data(), rdb::PixelLayout::kRgbaF32, static_cast<std::size_t>(count), 1,
+                static_cast<std::size_t>(count) * 16, count, false, gray);
+  if (t->tree.color_count() != count) {
+    const int kept = t->tree.color_count();
+    delete t;
+    return rdb::Fail(RDB_E_INVALID, std::string(path) + ": the tree reduced " +
+                                        std::to_string(count) + " colours to " +
+                                        std::to_string(kept) +
+                                        "; the palette holds duplicate or unreachable entries");
+  }
+  if (associate_alpha) *associate_alpha = assoc ? 1 : 0;
+  *out = t;
+  return RDB_OK;
+}
+
 int rdb_is_grayscale(const void* pixels, int layout, size_t width, size_t height,
                      size_t row_stride) {
   if (!pixels || !LayoutOk(layout)) return 0;

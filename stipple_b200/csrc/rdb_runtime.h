@@ -23,6 +23,12 @@ const char* LastError();
 std::size_t BytesPerPixel(int layout);
 // Bytes of one packed frame of an RDB_* format, 0 when unknown or invalid.
 std::size_t FrameBytes(int format, int width, int height);
+
+// Palette text files (rdb_palette_file.cpp).  ReadPaletteText returns the
+// sorted colours as a one-row RgbaF strip for the tree build.
+int WritePaletteText(const double* colors, int count, const std::string& path);
+int ReadPaletteText(const std::string& path, int expect_colors, std::vector<float>* strip,
+                    int* count, bool* associate_alpha, bool* grayscale);
 int Fail(int code, const std::string& msg);
 int CudaFail(cudaError_t e, const char* what);
 std::string CudaErr(cudaError_t e, const char* what);
