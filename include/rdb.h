@@ -154,11 +154,12 @@ int rdb_palette_from_octree(rdb_context* ctx, const rdb_octree* t, int* palette_
  * palette's device blocks return to the context's pool. */
 int rdb_palette_destroy(rdb_context* ctx, int palette_id);
 /* The palette's uniform-key table (stipple_b200/csrc/rdb_uniform.h) copied to
- * host memory: 2^18 bytes, one per 6-bit-per-channel memo key, holding the
- * colour number every target with that key receives, or 255 when the search
- * result can vary inside the key (or is colour 255).  Palettes without
- * associated alpha only.  No reference counterpart: it is how the sequential
- * engines skip the memo for such keys. */
+ * host memory: one byte per 6-bit-per-channel memo key, holding the colour
+ * number every target with that key receives, or 255 when the search result
+ * can vary inside the key (or is colour 255).  2^18 bytes; 2^24 for a palette
+ * that associates alpha (254 is then never a uniform colour either).  No
+ * reference counterpart: it is how the sequential engines skip the memo for
+ * such keys. */
 int rdb_palette_uniform(rdb_context* ctx, int palette_id, uint8_t* out, size_t cap);
 
 /* ---- dithering -----------------------------------------------------------

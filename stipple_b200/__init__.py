@@ -348,9 +348,10 @@ class Context:
     def release_palette(self, pid: int) -> None:
         _check(load().rdb_palette_destroy(self.handle, pid))
 
-    def uniform_table(self, pid: int) -> np.ndarray:
-        """The palette's uniform-key table: 2^18 bytes, 255 = not uniform."""
-        out = np.empty(1 << 18, np.uint8)
+    def uniform_table(self, pid: int, alpha: bool = False) -> np.ndarray:
+        """The palette's uniform-key table: 2^18 bytes (2^24 for a palette that
+        associates alpha), 255 = not uniform."""
+        out = np.empty(1 << (24 if alpha else 18), np.uint8)
         _check(load().rdb_palette_uniform(self.handle, pid, _ptr(out), out.nbytes))
         return out
 

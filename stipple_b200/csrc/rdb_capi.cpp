@@ -302,13 +302,24 @@ int rdb_palette_destroy(rdb_context* ctx, int palette_id) {
 
 int rdb_palette_uniform(rdb_context* ctx, int palette_id, uint8_t* out, size_t cap) {
   if (!ctx || !out) return Guard("rdb_palette_uniform");
-  if (cap < static_cast<size_t>(rdb::kUniformKeys)) {
-    return rdb::Fail(RDB_E_INVALID, "rdb_palette_uniform: buffer shorter than 2^18 bytes");
+  const rdb::DevPlan* p = ctx->impl.Plan(palette_id);
+  if (!p) return rdb::Fail(RDB_E_INVALID, "unknown palette id");
+  const size_t keys = p->assoc ? rdb::kUniformKeysAlpha : rdb::kUniformKeys;
+  if (cap < keys) {
+    return rdb::Fail(RDB_E_INVALID, p->assoc ? "rdb_palette_uniform: buffer shorter than 2^24 bytes"
+                                             : "rdb_palette_uniform: buffer shorter than 2^18 bytes");
   }
   cudaSetDevice(ctx->impl.device());
+  cudaStream_t s = ctx->impl.stream();
   const uint8_t* dev = nullptr;
-  if (int rc = ctx->impl.Uniform(palette_id, ctx->impl.stream(), &dev)) return rc;
-  const cudaError_t e = cudaMemcpy(out, dev, rdb::kUniformKeys, cudaMemcpyDeviceToHost);
+  if (int rc = ctx->impl.Uniform(palette_id, s, &dev)) return rc;
+  cudaError_t e = cudaSuccess;
+  if (p->assoc) {
+    // Classify every key the walks have not met yet.
+    e = rdb::LaunchUniformTableAlpha(p->dev, const_cast<uint8_t*>(dev), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dev, keys, cudaMemcpyDeviceToHost);
   return e == cudaSuccess ? RDB_OK : rdb::CudaFail(e, "rdb_palette_uniform");
 }
 

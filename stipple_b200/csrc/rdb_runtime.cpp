@@ -271,7 +271,7 @@ int Context::DestroyPalette(int id) {
   if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
   cudaStreamSynchronize(stream_);
   FreeBlock(it->second.dev, it->second.dev_bytes);
-  FreeBlock(it->second.uniform, kUniformKeys);
+  FreeBlock(it->second.uniform, it->second.assoc ? kUniformKeysAlpha : kUniformKeys);
   plans_.erase(it);
   return RDB_OK;
 }
@@ -280,7 +280,22 @@ int Context::Uniform(int id, cudaStream_t s, const uint8_t** out) {
   auto it = plans_.find(id);
   if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
   DevPlan& p = it->second;
-  if (p.assoc) return Fail(RDB_E_UNSUPPORTED, "uniform-key table: alpha-associated palette");
+  if (p.assoc) {
+    // 2^24 keys, classified lazily: every entry starts "not yet classified"
+    // and the segmented walk classifies the keys it meets after each pass.
+    if (!p.uniform) {
+      int rc = RDB_OK;
+      p.uniform = static_cast<uint8_t*>(AllocBlock(kUniformKeysAlpha, "uniform-key table", &rc));
+      if (!p.uniform) return rc;
+      cudaError_t e;
+      if ((e = cudaMemsetAsync(p.uniform, kUniformUnknown, kUniformKeysAlpha, s)) != cudaSuccess ||
+          (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        return CudaFail(e, "uniform-key table");
+      }
+    }
+    *out = p.uniform;
+    return RDB_OK;
+  }
   if (!p.uniform) {
     int rc = RDB_OK;
     p.uniform = static_cast<uint8_t*>(AllocBlock(kUniformKeys, "uniform-key table", &rc));
@@ -1207,8 +1222,11 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     im.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
     im.plan = p->dev;
     im.plan_smem = p->smem;
-    if (!assoc) {
-      if (int rc = Uniform(j.palette_id, s, &im.uni)) return rc;
+    if (int rc = Uniform(j.palette_id, s, &im.uni)) {
+      // An alpha palette's table is an accelerator: without room for it the
+      // walk answers every key through the memo.
+      if (!assoc) return rc;
+      im.uni = nullptr;
     }
     im.first_seg = total;
     im.nsegs = (im.n + seg_len - 1) / seg_len;
@@ -1437,7 +1455,8 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
           (e = cudaEventRecord(pass_ev_[k], s)) != cudaSuccess) {
         return drain(RDB_E_CUDA, CudaErr(e, "verification readback"));
       }
-      if (profiling_) stats_.launches += 1 + 1 + (use_cache ? 2 : 0);  // walk, checks, [prepare, keys]
+      // walk, checks, [prepare, keys, alpha-key classification]
+      if (profiling_) stats_.launches += 1 + 1 + (use_cache ? (assoc ? 3 : 2) : 0);
       ++issued;
     }
     if (checked == issued) return drain(RDB_E_DEVICE, "segmented walk did not converge within the pass limit");

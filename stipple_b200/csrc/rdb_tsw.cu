@@ -11,6 +11,7 @@
 #include "rdb_device.cuh"
 #include "rdb_tsw.h"
 #include "rdb_uniform.h"
+#include "rdb_uniform_alpha.cuh"
 #include "rdb_walk_thread.cuh"
 
 namespace rdb {
@@ -19,6 +20,7 @@ namespace {
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kNoUser = 0xFFFFFFFFu;
 constexpr int kKeys = 1 << 18;
+constexpr int kFillBlocks = 64;  // per image: the classification kernel's grid
 
 __device__ __forceinline__ int front_of(const TswLaunch& L, int image, int nsegs) {
   const int b = L.bad[(L.pass & 1) ^ 1][image];
@@ -297,7 +299,13 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
       uint8_t uv = kNotUniform;
       uint32_t gv = kNone;
       if constexpr (kAssoc) {
-        if (keyed) {
+        // Keys the table has classified uniform need no memo; keys not yet
+        // classified, and the rest, go through the hashed map.
+        if (uni) {
+          uv = __ldg(uni + key);
+          if (uv == kUniformUnknown) uv = kNotUniform;
+        }
+        if (keyed && uv == kNotUniform) {
           slot = map_find(hkeys, hmask, key, &present);
           if (present) gv = __ldg(gprev + slot);
         }
@@ -474,6 +482,25 @@ __global__ void TswPrepare(TswLaunch L) {
     const uint32_t gv = gp[slot];
     gn[slot] = (gv != kNone && static_cast<int>(gv >> 8) < front) ? gv : kNone;
     im.usemin[slot] = kNoUser;
+  }
+}
+
+// Classifies the keys of alpha-associated palettes that this pass's walk met
+// for the first time (every key it booked is in the image's hashed map):
+// rdb_uniform_alpha.cuh.  Later passes then answer the uniform ones without
+// the memo.  Images sharing a palette write the same values.
+__global__ void TswUniformFill(TswLaunch L) {
+  const int m = blockIdx.y;
+  if (m >= L.n_images) return;
+  const TswImage& im = L.images[m];
+  if (!im.hkeys || !im.uni) return;
+  uint8_t* table = const_cast<uint8_t*>(im.uni);
+  const int n = *im.hcount;
+  tw::Plan P;
+  P.bind(im.plan);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned key = im.hkeys[im.hlist[i]] - 1u;
+    if (table[key] == kUniformUnknown) table[key] = uniform_alpha_key(P, key);
   }
 }
 
@@ -657,6 +684,10 @@ cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) 
     TswVerifyKeys<<<dim3(kKeys / 256, L.n_images), 256, 0, s>>>(L);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (L.assoc) {
+      TswUniformFill<<<dim3(kFillBlocks, L.n_images), 256, 0, s>>>(L);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
   }
   if (total_segs <= 0) return cudaSuccess;
   TswVerifySegments<<<(total_segs + 7) / 8, 256, 0, s>>>(L, total_segs);
@@ -715,6 +746,11 @@ cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int tota
     e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifyKeys), dim3(kKeys / 256, L->n_images),
                   dim3(256), 0, args1);
     if (e != cudaSuccess) return e;
+    if (L->assoc) {
+      e = AddKernel(g, last, reinterpret_cast<const void*>(TswUniformFill),
+                    dim3(kFillBlocks, L->n_images), dim3(256), 0, args1);
+      if (e != cudaSuccess) return e;
+    }
   }
   if (total_segs > 0) {
     void* args2[] = {L, &total_segs};

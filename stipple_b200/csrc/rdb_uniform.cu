@@ -3,6 +3,7 @@
 
 #include "rdb_device.cuh"
 #include "rdb_uniform.h"
+#include "rdb_uniform_alpha.cuh"
 #include "rdb_walk_thread.cuh"
 
 namespace rdb {
@@ -77,7 +78,21 @@ __global__ void UniformKernel(const unsigned char* plan, uint8_t* out) {
   out[key] = P.seq[win];
 }
 
+// Every key of an alpha-associated palette's table still marked unknown.
+__global__ void UniformAlphaKernel(const unsigned char* plan, uint8_t* out) {
+  const unsigned key = blockIdx.x * blockDim.x + threadIdx.x;
+  if (key >= static_cast<unsigned>(kUniformKeysAlpha) || out[key] != kUniformUnknown) return;
+  tw::Plan P;
+  P.bind(plan);
+  out[key] = uniform_alpha_key(P, key);
+}
+
 }  // namespace
+
+cudaError_t LaunchUniformTableAlpha(const unsigned char* plan, uint8_t* out, cudaStream_t s) {
+  UniformAlphaKernel<<<kUniformKeysAlpha / 256, 256, 0, s>>>(plan, out);
+  return cudaGetLastError();
+}
 
 cudaError_t LaunchUniformTable(const unsigned char* plan, uint8_t* out, cudaStream_t s) {
   UniformKernel<<<kUniformKeys / 256, 256, 0, s>>>(plan, out);

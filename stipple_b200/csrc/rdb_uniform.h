@@ -30,8 +30,14 @@ namespace rdb {
 
 constexpr int kUniformKeys = 1 << 18;
 constexpr uint8_t kNotUniform = 0xFF;
+constexpr int kUniformKeysAlpha = 1 << 24;  // alpha-associated palettes (rdb_uniform_alpha.cuh)
+constexpr uint8_t kUniformUnknown = 0xFE;   // their lazily filled entries: not yet classified
 
 // `plan`: a device plan blob (rdb_plan.h); `out`: kUniformKeys bytes.
 cudaError_t LaunchUniformTable(const unsigned char* plan, uint8_t* out, cudaStream_t s);
+
+// Alpha-associated palettes (rdb_uniform_alpha.cuh): 2^24 bytes, classified
+// lazily by the walk (0xFE = not yet); this classifies every key still 0xFE.
+cudaError_t LaunchUniformTableAlpha(const unsigned char* plan, uint8_t* out, cudaStream_t s);
 
 }  // namespace rdb
