@@ -58,7 +58,9 @@ std::size_t EstimateBytes(const rdb_request& r) {
   const std::size_t px = static_cast<std::size_t>(r.width) * r.height;
   std::size_t b = px * (rdb::BytesPerPixel(r.layout) + 1 + (r.rgba_out ? 16 : 0)) + 4 * px;
   if (r.engine == RDB_ENGINE_SEQ) {
-    b += px * 64 + (std::size_t{3} << 20) + (r.associate_alpha ? px * 16 : 0);
+    // Scratch and key maps; an alpha-associated palette also holds its
+    // 2^24-byte uniform-key table while the request is on the device.
+    b += px * 64 + (std::size_t{3} << 20) + (r.associate_alpha ? px * 16 + (std::size_t{1} << 24) : 0);
   } else {
     b += px * 24;
   }
