@@ -371,10 +371,13 @@ void rdb_server_destroy(rdb_server* s);
  * Limits: at most 4096 pixels per side and 1048576 pixels, palettes without
  * associated alpha (an alpha memo has 2^24 keys), plan blob <= 64 KiB; larger
  * inputs are refused with RDB_E_UNSUPPORTED and a message.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture on the device.  The work is
- * enqueued on `stream` (NULL = legacy default stream); device-side status is
- * not reported.  All calls share the one array and it keeps the last call's
+ * device looks up the array's device address (cudaGetSymbolAddress) and keeps
+ * it for the life of the process, so make that first call before any stream
+ * capture on the device, and do not use this entry point on a device after
+ * cudaDeviceReset (the address it kept is then stale).  The work is enqueued on
+ * `stream` (NULL = legacy default stream); device-side status is not reported.
+ * `plan` is copied on `stream`: keep it valid and unchanged until the stream
+ * reaches the call (from pinned memory that copy is asynchronous).  All calls share the one array and it keeps the last call's
  * contents (the memo table is told apart by a generation counter, the work
  * counter is cleared each call), so calls that overlap on the GPU -- on
  * different streams, or from different threads -- race and corrupt each

@@ -55,8 +55,6 @@ def _obj(src: str) -> str:
 def _compile(src: str, ptxas_verbose: bool) -> tuple[str, str]:
     path = os.path.join(CSRC, src)
     cmd = [NVCC, *ARCH, *COMMON, *DEVICE, "-c", path, "-o", _obj(src)]
-    if src.endswith(".cpp"):
-        cmd[1:1] = ["-x", "cu"] if False else []
     if ptxas_verbose and src.endswith(".cu"):
         cmd.append("-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -89,7 +87,10 @@ def _lib_current() -> bool:
 # The reference-facing C++ layer (stipple_b200/dropin) is compiled against
 # the reference's own headers, where that tree is present; elsewhere the
 # libraries built here earlier are used as they are.
-REFERENCE = os.environ.get("RDB_REFERENCE", "/root/reference")
+# The reference checkout: $RDB_REFERENCE, else a sibling of this repository
+# named "reference".
+REFERENCE = os.environ.get("RDB_REFERENCE",
+                           os.path.normpath(os.path.join(ROOT, os.pardir, "reference")))
 DROPIN = os.path.join(HERE, "dropin")
 DROPIN_LIB = os.path.join(LIBDIR, "librd_b200_dropin.so")
 PLUGIN_LIB = os.path.join(LIBDIR, "librd_b200_plugin.so")

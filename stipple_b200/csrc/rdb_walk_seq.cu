@@ -348,6 +348,17 @@ cudaError_t Base(int device, unsigned char** out) {
   return cudaSuccess;
 }
 
+// Writes the call's launch descriptor into the array and clears the work
+// counter and the status word.  The descriptor travels as a kernel parameter,
+// so no host buffer of the call has to outlive it.
+__global__ void Stage(SeqItem item, SeqItem* dst, uint32_t* misc) {
+  if (threadIdx.x == 0) {
+    *dst = item;
+    misc[1] = 0u;
+    misc[2] = 0u;
+  }
+}
+
 }  // namespace noalloc
 
 }  // namespace rdb
@@ -416,13 +427,14 @@ extern "C" int rdb_dither_seq_noalloc(const void* plan, size_t plan_bytes, const
   item.plan = dplan;
   item.plan_smem = h.smem_bytes;
   // The counter and status start at zero on every call; the memo slab keeps
-  // its contents and is told apart by the generation in misc[0].
-  if ((e = cudaMemsetAsync(misc + 1, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(dplan, plan, plan_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(base + na::kOffItem, &item, sizeof(item), cudaMemcpyHostToDevice, s)) !=
-          cudaSuccess) {
-    return CudaFail(e, "rdb_dither_seq_noalloc staging");
+  // its contents and is told apart by the generation in misc[0].  The plan is
+  // copied from the caller's buffer, which must stay unchanged until the
+  // stream reaches this call (from pinned memory the copy is asynchronous).
+  if ((e = cudaMemcpyAsync(dplan, plan, plan_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+    return CudaFail(e, "rdb_dither_seq_noalloc plan copy");
   }
+  na::Stage<<<1, 32, 0, s>>>(item, reinterpret_cast<SeqItem*>(base + na::kOffItem), misc);
+  if ((e = cudaGetLastError()) != cudaSuccess) return CudaFail(e, "rdb_dither_seq_noalloc staging");
   if ((e = BuildSeqOrder(width, height, order, base + na::kOffCurve, na::kCurveBytes, s)) != cudaSuccess) {
     return CudaFail(e, "visit order kernel");
   }

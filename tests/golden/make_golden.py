@@ -209,4 +209,4 @@ def main(ref_dir: str) -> None:
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    main(args[0] if args else "/root/reference")
+    main(args[0] if args else os.path.normpath(os.path.join(ROOT, "..", "reference")))

@@ -46,6 +46,9 @@ def test_noalloc_matches_rdb_dither_twice(lib):
             d_img = torch.from_numpy(img).cuda()
             for call in range(2):
                 d_idx = torch.full((h, w), 7, dtype=torch.uint8, device="cuda")
+                # The fill above ran on torch's current stream; the walk runs on
+                # `stream`, so order the two.
+                stream.wait_stream(torch.cuda.current_stream())
                 rc = lib.rdb_dither_seq_noalloc(blob.ctypes.data, blob.size, d_img.data_ptr(), 0,
                                                 w, h, sb.RGB8, d_idx.data_ptr(), 1.0, 1,
                                                 C.c_void_p(stream.cuda_stream))
@@ -53,6 +56,38 @@ def test_noalloc_matches_rdb_dither_twice(lib):
                 stream.synchronize()
                 got = d_idx.cpu().numpy()
                 assert np.array_equal(got, want), (w, h, colors, call)
+    finally:
+        ctx.close()
+
+
+def test_noalloc_generation_wrap(lib):
+    """The memo table in the shared array is told apart between calls by an
+    8-bit generation that wraps after 255 calls, when the table is cleared.
+    Enough calls on a small image to pass the wrap; the last ones are checked
+    bit for bit against rdb_dither."""
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    ctx = sb.Context(0)
+    try:
+        w, h = 16, 16
+        img = synth.gradient_rgb8(w, h, 11)
+        tree = sb.Octree(img, 16, False)
+        pid = ctx.palette_from_octree(tree)
+        want = ctx.dither_host("seq", img, pid)
+        ctx.release_palette(pid)
+        blob = np.frombuffer(_plan(tree), np.uint8).copy()
+        d_img = torch.from_numpy(img).cuda()
+        d_idx = torch.full((h, w), 7, dtype=torch.uint8, device="cuda")
+        stream.wait_stream(torch.cuda.current_stream())
+        for call in range(262):
+            rc = lib.rdb_dither_seq_noalloc(blob.ctypes.data, blob.size, d_img.data_ptr(), 0,
+                                            w, h, sb.RGB8, d_idx.data_ptr(), 1.0, 1,
+                                            C.c_void_p(stream.cuda_stream))
+            assert rc == 0, lib.rdb_last_error().decode()
+            if call >= 250:
+                stream.synchronize()
+                assert np.array_equal(d_idx.cpu().numpy(), want), call
     finally:
         ctx.close()
 
