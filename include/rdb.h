@@ -85,11 +85,24 @@ void rdb_octree_free(rdb_octree* t);
  * greyscale when every row is grey) -- refused if it merges any.  The tree's
  * colormap is then the palette; `associate_alpha` receives 1 when some row's
  * alpha is not opaque (the reference's palette flag).  `expect_colors` > 0
- * refuses a file with another count.  Other extensions (the PNG form, which
- * is ImageMagick's PNG8 codec) return RDB_E_UNSUPPORTED. */
+ * refuses a file with another count.  Other extensions return
+ * RDB_E_UNSUPPORTED (the image form is rdb_palette_*_png). */
 int rdb_palette_write_text(const double* colors /* count x 4 */, int count, const char* path);
 int rdb_palette_read_text(const char* path, int expect_colors, rdb_octree** out,
                           int* associate_alpha);
+/* The image form of the same files, as PNG.  The writer is ImWritePalette's
+ * image branch (src/rd_im.cpp:1047-1118): a 1 x count strip of 8-bit colours,
+ * each channel narrowed by ImageMagick's ScaleQuantumToChar, as an indexed PNG
+ * (count <= 256).  The reader is ImReadPalette's image branch (:1362-1388)
+ * with ImAdoptPaletteFromColormap (:731-888): an indexed PNG gives its PLTE
+ * entries in order (alpha from tRNS), any other PNG its distinct RGB values in
+ * scan order; 8-bit samples scale by 257 to Q16; `expect_colors` > 0 must
+ * equal the colours the image holds; duplicates are dropped; the tree is
+ * built from a swatch (8 x 8 per colour, ceil(sqrt(n)) per row) with as many
+ * colours as entries, no alpha association, greyscale when every entry is
+ * grey.  The tree's colormap is the palette. */
+int rdb_palette_write_png(const double* colors /* count x 4 */, int count, const char* path);
+int rdb_palette_read_png(const char* path, int expect_colors, rdb_octree** out);
 /* 1 when every pixel has r == g == b (the reference's greyscale rule,
  * src/rd_cli.cpp:2452-2456). */
 int rdb_is_grayscale(const void* pixels, int layout, size_t width, size_t height,
@@ -126,6 +139,23 @@ typedef struct rdb_kernel_stats {
 } rdb_kernel_stats;
 int rdb_context_profile(rdb_context* ctx, int enable);
 int rdb_context_stats(const rdb_context* ctx, rdb_kernel_stats* out);
+
+/* Dependent latency in SM cycles of each operation on the sequential walk's
+ * per-step chain, measured on `device` by one thread timing chains of
+ * dependent operations with clock64().  A diagnostic for the chain-latency
+ * roofline; no reference counterpart. */
+typedef struct rdb_latency_table {
+  double dadd;            /* __dadd_rn */
+  double dmul;            /* __dmul_rn */
+  double f64_to_f32;      /* half of a double -> float -> double round trip */
+  double f32_to_f64;
+  double f32_to_int;      /* float -> int (truncating) */
+  double shared_load;     /* shared-memory pointer chase */
+  double global_load_l1;  /* global pointer chase hitting L1 */
+  double global_load_l2;  /* global pointer chase hitting L2 (L1 bypassed) */
+  double int_op;          /* integer add / xor */
+} rdb_latency_table;
+int rdb_probe_latency(int device, rdb_latency_table* out);
 
 /* A palette and its colour tree, in the reference's own terms
  * (rd::Palette, include/rd_riemersma.h:63-67; rd::QNode, include/rd_octree.h:43-52). */
@@ -305,7 +335,8 @@ typedef struct rdb_server_options {
   size_t memory_budget;   /* admission cap in bytes (0 = 90 % of free memory) */
   int workers;            /* device workers (0 = 4) */
   int max_batch;          /* requests per batch (0 = 512) */
-  int host_threads;       /* palette builders (0 = hardware threads) */
+  int host_threads;       /* palette builders (0 = the CPUs this process may run on:
+                             its affinity mask, capped by a cgroup CPU quota) */
 } rdb_server_options;
 
 typedef struct rdb_request {
@@ -331,6 +362,17 @@ typedef struct rdb_request_result {
   int batch_size;         /* requests in its batch */
 } rdb_request_result;
 
+/* Stages of a request's latency, in order (rdb_server_stats.stage_*). */
+enum {
+  RDB_STAGE_BUILD_WAIT = 0, /* submit -> a palette builder takes it */
+  RDB_STAGE_BUILD = 1,      /* octree build on the host */
+  RDB_STAGE_ADMIT = 2,      /* built -> a device worker starts its batch (memory admission,
+                               free worker) */
+  RDB_STAGE_DEVICE = 3,     /* the batch call: palette upload, H2D, walk, D2H */
+  RDB_STAGE_TOTAL = 4,      /* submit -> result in host memory */
+  RDB_STAGES = 5
+};
+
 typedef struct rdb_server_stats {
   int64_t completed;
   int64_t failed;
@@ -341,6 +383,10 @@ typedef struct rdb_server_stats {
   double max_ms;
   double mpx_per_s;       /* pixels / (last completion - first submission) */
   size_t peak_admitted_bytes;
+  double stage_p50_ms[RDB_STAGES]; /* per-stage percentiles (RDB_STAGE_*) */
+  double stage_p99_ms[RDB_STAGES];
+  int host_threads;       /* palette builders running */
+  int workers;            /* device workers running */
 } rdb_server_stats;
 
 int rdb_server_create(const rdb_server_options* opts, rdb_server** out);
@@ -350,6 +396,10 @@ int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket);
  * it is not done yet.  The ticket is released once waited for successfully. */
 int rdb_server_wait(rdb_server* s, uint64_t ticket, int timeout_ms, rdb_request_result* out);
 int rdb_server_stats_get(rdb_server* s, rdb_server_stats* out);
+/* Forgets the statistics gathered so far (latencies, counts, throughput span,
+ * peak admission), e.g. after a warm-up stream; requests in flight count
+ * toward the new window when they complete. */
+int rdb_server_stats_reset(rdb_server* s);
 /* Finishes everything submitted, then stops the threads. */
 void rdb_server_destroy(rdb_server* s);
 

@@ -79,7 +79,20 @@ class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_int64), ("failed", C.c_int64), ("pixels", C.c_int64),
                 ("batches", C.c_int64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("max_ms", C.c_double), ("mpx_per_s", C.c_double),
-                ("peak_admitted_bytes", C.c_size_t)]
+                ("peak_admitted_bytes", C.c_size_t), ("stage_p50_ms", C.c_double * 5),
+                ("stage_p99_ms", C.c_double * 5), ("host_threads", C.c_int), ("workers", C.c_int)]
+
+
+# Latency stages of a served request (RDB_STAGE_* in include/rdb.h).
+SERVER_STAGES = ("build_wait", "build", "admit", "device", "total")
+
+
+class LatencyTable(C.Structure):
+    """rdb_latency_table (include/rdb.h): cycles per dependent operation."""
+    _fields_ = [("dadd", C.c_double), ("dmul", C.c_double), ("f64_to_f32", C.c_double),
+                ("f32_to_f64", C.c_double), ("f32_to_int", C.c_double),
+                ("shared_load", C.c_double), ("global_load_l1", C.c_double),
+                ("global_load_l2", C.c_double), ("int_op", C.c_double)]
 
 
 class Job(C.Structure):
@@ -161,6 +174,10 @@ SIGNATURES = {
     "rdb_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
     "rdb_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p]),
     "rdb_server_stats_get": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rdb_server_stats_reset": (C.c_int, [C.c_void_p]),
+    "rdb_probe_latency": (C.c_int, [C.c_int, C.c_void_p]),
+    "rdb_palette_write_png": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
+    "rdb_palette_read_png": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "rdb_server_destroy": (None, [C.c_void_p]),
     "rdb_max_frames": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t]),
     "rdb_context_profile": (C.c_int, [C.c_void_p, C.c_int]),
@@ -531,6 +548,13 @@ def plan_blob(colors, child, color_number, number_unique, associate_alpha, paren
     return buf.tobytes()
 
 
+def probe_latency(device: int = 0) -> dict:
+    """rdb_probe_latency: the measured dependent-latency table (cycles)."""
+    t = LatencyTable()
+    _check(load().rdb_probe_latency(device, C.byref(t)))
+    return {f: getattr(t, f) for f, _ in LatencyTable._fields_}
+
+
 def device_count() -> int:
     c = C.c_int()
     rc = load().rdb_device_count(C.byref(c))
@@ -566,6 +590,37 @@ def read_palette_text(path: str, expect_colors: int = 0) -> tuple[Octree, bool]:
     return t, bool(assoc.value)
 
 
+def write_palette_png(colors: np.ndarray, path: str) -> None:
+    """rdither's palette image file as PNG (rdb_palette_write_png): a 1 x count
+    indexed strip of the 8-bit colours."""
+    c = np.ascontiguousarray(colors, np.float64).reshape(-1, 4)
+    _check(load().rdb_palette_write_png(_ptr(c), c.shape[0], path.encode()))
+
+
+def read_palette_png(path: str, expect_colors: int = 0) -> Octree:
+    """Reads a palette image file (rdb_palette_read_png): the tree built from
+    its colours."""
+    t = Octree(None)
+    _check(load().rdb_palette_read_png(path.encode(), int(expect_colors), C.byref(t.handle)))
+    return t
+
+
+def write_palette(colors: np.ndarray, path: str) -> None:
+    """--palette-export: the text form for .txt / .text paths, else the PNG strip."""
+    if path.endswith((".txt", ".text")):
+        write_palette_text(colors, path)
+    else:
+        write_palette_png(colors, path)
+
+
+def read_palette(path: str, expect_colors: int = 0) -> tuple[Octree, bool]:
+    """--palette-from: the text form for .txt / .text paths, else a PNG (an image
+    palette never associates alpha)."""
+    if path.endswith((".txt", ".text")):
+        return read_palette_text(path, expect_colors)
+    return read_palette_png(path, expect_colors), False
+
+
 def frame_bytes(fmt: int, width: int, height: int) -> int:
     """Bytes of one packed frame of `fmt` (0 when unknown or invalid)."""
     return int(load().rdb_frame_bytes(fmt, width, height))
@@ -589,13 +644,17 @@ class Server:
 
     def submit(self, img: np.ndarray, colors: int, engine: str | int = "seq",
                alpha: bool = False, rgba: bool = False, **opts) -> int:
-        img = np.ascontiguousarray(img)
+        # A crop of a larger image is submitted in place (its rows are
+        # contiguous; the row stride says how far apart they are).
+        if not (img.ndim == 3 and img.strides[2] == img.itemsize and
+                img.strides[1] == img.shape[2] * img.itemsize and img.strides[0] > 0):
+            img = np.ascontiguousarray(img)
         h, w = img.shape[:2]
-        idx = np.zeros((h, w), np.uint8)
+        idx = np.empty((h, w), np.uint8)
         out = np.zeros((h, w, 4), np.float32) if rgba else None
         r = Request()
-        r.pixels = _ptr(img)
-        r.row_stride = 0
+        r.pixels = img.__array_interface__["data"][0]
+        r.row_stride = img.strides[0]
         r.width, r.height, r.layout = w, h, layout_of(img)
         r.colors = colors
         r.associate_alpha = int(alpha)
@@ -621,7 +680,14 @@ class Server:
     def stats(self) -> dict:
         st = ServerStats()
         _check(load().rdb_server_stats_get(self.handle, C.byref(st)))
-        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+        out = {f: getattr(st, f) for f, _ in ServerStats._fields_}
+        out["stages"] = {name: {"p50_ms": st.stage_p50_ms[i], "p99_ms": st.stage_p99_ms[i]}
+                         for i, name in enumerate(SERVER_STAGES)}
+        del out["stage_p50_ms"], out["stage_p99_ms"]
+        return out
+
+    def reset_stats(self) -> None:
+        _check(load().rdb_server_stats_reset(self.handle))
 
     def close(self) -> None:
         if self.handle:

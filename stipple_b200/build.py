@@ -38,6 +38,7 @@ SOURCES = [
     "rdb_capi.cpp",
     "rdb_serve.cpp",
     "rdb_palette_file.cpp",
+    "rdb_palette_png.cpp",
     "rdb_curve.cu",
     "rdb_walk_seq.cu",
     "rdb_walk_blocks.cu",
@@ -45,6 +46,8 @@ SOURCES = [
     "rdb_ssw.cu",
     "rdb_tsw.cu",
     "rdb_uniform.cu",
+    "rdb_probe.cu",
+    "rdb_cand.cu",
 ]
 
 
@@ -135,7 +138,8 @@ def build(ptxas_verbose: bool = False, force: bool = False) -> str:
                 if log.strip():
                     logs.append(f"--- {src}\n{log}")
     if todo or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *[_obj(s) for s in SOURCES], "-lcudart"]
+        # zlib: the PNG form of palette files.
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *[_obj(s) for s in SOURCES], "-lcudart", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

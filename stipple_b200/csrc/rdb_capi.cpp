@@ -173,6 +173,26 @@ int rdb_palette_read_text(const char* path, int expect_colors, rdb_octree** out,
   return RDB_OK;
 }
 
+int rdb_palette_write_png(const double* colors, int count, const char* path) {
+  if (!colors || !path) return Guard("rdb_palette_write_png");
+  return rdb::WritePalettePng(colors, count, path);
+}
+
+int rdb_palette_read_png(const char* path, int expect_colors, rdb_octree** out) {
+  if (!path || !out) return Guard("rdb_palette_read_png");
+  *out = nullptr;
+  std::vector<float> swatch;
+  std::size_t w = 0, h = 0;
+  int count = 0;
+  bool gray = false;
+  if (int rc = rdb::ReadPalettePng(path, expect_colors, &swatch, &w, &h, &count, &gray)) return rc;
+  rdb_octree* t = new (std::nothrow) rdb_octree();
+  if (!t) return rdb::Fail(RDB_E_NOMEM, "octree allocation");
+  t->tree.Build(swatch.data(), rdb::PixelLayout::kRgbaF32, w, h, w * 16, count, false, gray);
+  *out = t;
+  return RDB_OK;
+}
+
 int rdb_is_grayscale(const void* pixels, int layout, size_t width, size_t height,
                      size_t row_stride) {
   if (!pixels || !LayoutOk(layout)) return 0;

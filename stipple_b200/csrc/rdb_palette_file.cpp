@@ -37,8 +37,8 @@ int WritePaletteText(const double* colors, int count, const std::string& path) {
   if (count <= 0) return Fail(RDB_E_INVALID, "palette is empty");
   if (!PaletteTextPath(path)) {
     return Fail(RDB_E_UNSUPPORTED,
-                "only the text palette form (.txt / .text) is provided; the PNG form is "
-                "ImageMagick's PNG8 codec");
+                "the text palette form takes .txt / .text paths; write the image form with "
+                "rdb_palette_write_png");
   }
   FILE* f = std::fopen(path.c_str(), "wb");
   if (!f) return Fail(RDB_E_INVALID, "cannot open " + path + " for writing");
@@ -58,8 +58,8 @@ int ReadPaletteText(const std::string& path, int expect_colors, std::vector<floa
                     int* count, bool* associate_alpha, bool* grayscale) {
   if (!PaletteTextPath(path)) {
     return Fail(RDB_E_UNSUPPORTED,
-                "only the text palette form (.txt / .text) is provided; the PNG form is "
-                "ImageMagick's PNG8 codec");
+                "the text palette form takes .txt / .text paths; read the image form with "
+                "rdb_palette_read_png");
   }
   FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) return Fail(RDB_E_INVALID, "cannot open " + path + " for reading");

@@ -12,6 +12,7 @@
 #include "rdb_numeric.h"
 #include "rdb_ssw.h"
 #include "rdb_tsw.h"
+#include "rdb_cand.h"
 #include "rdb_uniform.h"
 
 namespace rdb {
@@ -272,6 +273,7 @@ int Context::DestroyPalette(int id) {
   cudaStreamSynchronize(stream_);
   FreeBlock(it->second.dev, it->second.dev_bytes);
   FreeBlock(it->second.uniform, it->second.assoc ? kUniformKeysAlpha : kUniformKeys);
+  FreeBlock(it->second.cand, kCandKeys * sizeof(uint32_t));
   plans_.erase(it);
   return RDB_OK;
 }
@@ -308,6 +310,26 @@ int Context::Uniform(int id, cudaStream_t s, const uint8_t** out) {
     }
   }
   *out = p.uniform;
+  return RDB_OK;
+}
+
+int Context::Candidates(int id, cudaStream_t s, const uint32_t** out) {
+  auto it = plans_.find(id);
+  if (it == plans_.end()) return Fail(RDB_E_INVALID, "unknown palette id");
+  DevPlan& p = it->second;
+  if (p.assoc) return Fail(RDB_E_INVALID, "candidate tables cover palettes without associated alpha");
+  if (!p.cand) {
+    int rc = RDB_OK;
+    p.cand = static_cast<uint32_t*>(AllocBlock(kCandKeys * sizeof(uint32_t), "candidate table", &rc));
+    if (!p.cand) return rc;
+    // Built once; other streams may read it later, so it is complete on return.
+    cudaError_t e;
+    if ((e = LaunchCandidateTable(p.dev, p.cand, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+      return CudaFail(e, "candidate table");
+    }
+  }
+  *out = p.cand;
   return RDB_OK;
 }
 
@@ -564,6 +586,7 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
   std::vector<BlockImage> imgs;
   std::vector<int64_t> offs;
   int64_t blocks = 0, positions = 0;
+  int64_t longest = 0;
   for (BlockImage b : all) {
     const int64_t nb = BlockListLength(b.width, b.height);
     if (nb == 0) {
@@ -578,16 +601,24 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
     b.nblocks = static_cast<int>((nb + o.block - 1) / o.block);
     blocks += b.nblocks;
     offs.push_back(positions);
-    positions += (nb + 15) & ~int64_t{15};
+    positions += nb;
+    longest = std::max(longest, nb);
     imgs.push_back(b);
   }
   if (imgs.empty()) return RDB_OK;
   const bool packed = layout == RDB_RGB8 || layout == RDB_RGBA8;
   const std::size_t word = packed ? 4 : 16;
+  // The walk's scratch (rdb_walk.h): groups of 32 blocks, bpad positions each.
+  const int bpad = static_cast<int>((std::min<int64_t>(o.block, longest) + 15) & ~int64_t{15});
+  const std::size_t cells = static_cast<std::size_t>((blocks + 31) / 32 * 32) * static_cast<std::size_t>(bpad);
   if (int rc = Reserve(&block_images_, imgs.size() * sizeof(BlockImage), "block images")) return rc;
   if (int rc = Reserve(&block_offsets_, offs.size() * sizeof(int64_t), "block offsets")) return rc;
-  if (int rc = Reserve(&block_cx_, static_cast<std::size_t>(positions) * word, "block samples")) return rc;
-  if (int rc = Reserve(&block_chosen_, static_cast<std::size_t>(positions), "block indices")) return rc;
+  if (int rc = Reserve(&block_cx_, cells * word, "block samples")) return rc;
+  if (int rc = Reserve(&block_chosen_, cells, "block indices")) return rc;
+  const uint32_t* cand = nullptr;
+  if (!p->assoc) {
+    if (int rc = Candidates(pid, s, &cand)) return rc;
+  }
   cudaMemcpyAsync(block_images_.ptr, imgs.data(), imgs.size() * sizeof(BlockImage),
                   cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(block_offsets_.ptr, offs.data(), offs.size() * sizeof(int64_t),
@@ -601,7 +632,9 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
   L.total_blocks = blocks;
   L.cx = static_cast<uint32_t*>(block_cx_.ptr);
   L.chosen = static_cast<uint8_t*>(block_chosen_.ptr);
-  L.cx_offset = static_cast<int64_t*>(block_offsets_.ptr);
+  L.pos_offset = static_cast<const int64_t*>(block_offsets_.ptr);
+  L.cand = cand;
+  L.bpad = bpad;
   L.plan = p->dev;
   L.plan_smem = p->smem;
   L.assoc = p->assoc ? 1 : 0;

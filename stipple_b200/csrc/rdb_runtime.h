@@ -27,6 +27,11 @@ std::size_t FrameBytes(int format, int width, int height);
 // Palette text files (rdb_palette_file.cpp).  ReadPaletteText returns the
 // sorted colours as a one-row RgbaF strip for the tree build.
 int WritePaletteText(const double* colors, int count, const std::string& path);
+// Palette PNG strips (rdb_palette_png.cpp).  ReadPalettePng returns the RgbaF
+// swatch image the tree is built from, its size, and the colour count.
+int WritePalettePng(const double* colors, int count, const std::string& path);
+int ReadPalettePng(const std::string& path, int expect_colors, std::vector<float>* swatch,
+                   std::size_t* width, std::size_t* height, int* count, bool* grayscale);
 int ReadPaletteText(const std::string& path, int expect_colors, std::vector<float>* strip,
                     int* count, bool* associate_alpha, bool* grayscale);
 int Fail(int code, const std::string& msg);
@@ -47,6 +52,7 @@ struct DevPlan {
   int count = 0;
   bool assoc = false;
   uint8_t* uniform = nullptr;  // uniform-key table (rdb_uniform.h), built on first use
+  uint32_t* cand = nullptr;    // candidate table (rdb_cand.h), built on first use
 };
 
 // Segment-length autotuner of the segmented walk: per (device, log2 of the
@@ -74,6 +80,9 @@ class Context {
   const DevPlan* Plan(int id) const;
   // The palette's uniform-key table, built on the stream on first use.
   int Uniform(int id, cudaStream_t s, const uint8_t** out);
+  // The palette's candidate table (rdb_cand.h); palettes without associated
+  // alpha only.
+  int Candidates(int id, cudaStream_t s, const uint32_t** out);
 
   // Visit order of a geometry, built on first use and kept resident.
   int Order(int width, int height, cudaStream_t s, const int32_t** out);

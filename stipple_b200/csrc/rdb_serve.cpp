@@ -16,9 +16,13 @@
 //            whichever worker frees first.
 // A request's result does not depend on its batch: every engine treats the
 // jobs of a call independently.
+#include <sched.h>
+
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -38,10 +42,43 @@ double Ms(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+// CPUs this process may run on: its affinity mask, capped by a cgroup (v2 or
+// v1) CPU quota when one is set.  hardware_concurrency() counts every CPU of
+// the machine, which oversubscribes a container limited to a few of them.
+int UsableCpus() {
+  int n = 0;
+  cpu_set_t set;
+  CPU_ZERO(&set);
+  if (sched_getaffinity(0, sizeof(set), &set) == 0) n = CPU_COUNT(&set);
+  if (n <= 0) n = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+  double quota = -1.0;
+  if (FILE* f = std::fopen("/sys/fs/cgroup/cpu.max", "r")) {
+    char q[64] = {0};
+    long long period = 0;
+    if (std::fscanf(f, "%63s %lld", q, &period) == 2 && std::strcmp(q, "max") != 0 && period > 0) {
+      quota = std::atof(q) / static_cast<double>(period);
+    }
+    std::fclose(f);
+  } else if (FILE* f1 = std::fopen("/sys/fs/cgroup/cpu/cpu.cfs_quota_us", "r")) {
+    long long qu = -1, period = 0;
+    if (std::fscanf(f1, "%lld", &qu) == 1 && qu > 0) {
+      if (FILE* f2 = std::fopen("/sys/fs/cgroup/cpu/cpu.cfs_period_us", "r")) {
+        if (std::fscanf(f2, "%lld", &period) == 1 && period > 0) {
+          quota = static_cast<double>(qu) / static_cast<double>(period);
+        }
+        std::fclose(f2);
+      }
+    }
+    std::fclose(f1);
+  }
+  if (quota > 0.0) n = std::min(n, std::max(1, static_cast<int>(quota + 0.5)));
+  return std::max(1, n);
+}
+
 struct Req {
   rdb_request r{};
   uint64_t ticket = 0;
-  Clock::time_point t_submit, t_built, t_start, t_done;
+  Clock::time_point t_submit, t_build_start, t_built, t_start, t_done;
   rdb_octree* tree = nullptr;
   std::size_t bytes = 0;
   int status = RDB_OK;
@@ -86,8 +123,8 @@ struct rdb_server {
   bool stop = false;
   int pending = 0;  // submitted, not yet completed
   std::vector<std::thread> builders, workers;
-  // statistics
-  std::vector<double> latencies;
+  // statistics: per completed request, its stage durations (RDB_STAGE_*)
+  std::vector<std::array<double, RDB_STAGES>> latencies;
   int64_t failed = 0, pixels = 0, batches = 0;
   bool any = false;
   Clock::time_point first_submit, last_done;
@@ -107,6 +144,7 @@ void rdb_server::Build() {
       if (incoming.empty()) return;
       q = incoming.front();
       incoming.pop_front();
+      q->t_build_start = Clock::now();
     }
     const rdb_request& r = q->r;
     const int gray = rdb_is_grayscale(r.pixels, r.layout, r.width, r.height, r.row_stride);
@@ -218,7 +256,8 @@ void rdb_server::Work(int index) {
       admitted -= q->bytes;
       --pending;
       if (rc == RDB_OK) {
-        latencies.push_back(Ms(q->t_submit, t1));
+        latencies.push_back({Ms(q->t_submit, q->t_build_start), Ms(q->t_build_start, q->t_built),
+                             Ms(q->t_built, t0), Ms(t0, t1), Ms(q->t_submit, t1)});
         pixels += static_cast<int64_t>(q->r.width) * q->r.height;
         last_done = t1;
       } else {
@@ -238,7 +277,7 @@ int rdb_server_create(const rdb_server_options* opts, rdb_server** out) {
   rdb_server* s = new rdb_server();
   if (opts) s->o = *opts;
   if (s->o.workers <= 0) s->o.workers = 4;
-  if (s->o.host_threads <= 0) s->o.host_threads = std::max(1u, std::thread::hardware_concurrency());
+  if (s->o.host_threads <= 0) s->o.host_threads = UsableCpus();
   if (cudaSetDevice(s->o.device) != cudaSuccess) {
     delete s;
     return rdb::Fail(RDB_E_CUDA, "rdb_server_create: no such device");
@@ -326,19 +365,38 @@ int rdb_server_stats_get(rdb_server* s, rdb_server_stats* out) {
   out->pixels = s->pixels;
   out->batches = s->batches;
   out->peak_admitted_bytes = s->peak;
+  out->host_threads = s->o.host_threads;
+  out->workers = s->o.workers;
   if (!s->latencies.empty()) {
-    std::vector<double> v = s->latencies;
-    std::sort(v.begin(), v.end());
+    std::vector<double> v(s->latencies.size());
     const auto pct = [&](double p) {
       const std::size_t k = static_cast<std::size_t>(p * static_cast<double>(v.size() - 1) + 0.5);
       return v[std::min(k, v.size() - 1)];
     };
-    out->p50_ms = pct(0.50);
-    out->p99_ms = pct(0.99);
+    for (int st = 0; st < RDB_STAGES; ++st) {
+      for (std::size_t i = 0; i < v.size(); ++i) v[i] = s->latencies[i][static_cast<std::size_t>(st)];
+      std::sort(v.begin(), v.end());
+      out->stage_p50_ms[st] = pct(0.50);
+      out->stage_p99_ms[st] = pct(0.99);
+    }
+    out->p50_ms = out->stage_p50_ms[RDB_STAGE_TOTAL];
+    out->p99_ms = out->stage_p99_ms[RDB_STAGE_TOTAL];
     out->max_ms = v.back();
     const double span = Ms(s->first_submit, s->last_done);
     out->mpx_per_s = span > 0 ? static_cast<double>(s->pixels) / (span * 1e3) : 0.0;
   }
+  return RDB_OK;
+}
+
+int rdb_server_stats_reset(rdb_server* s) {
+  if (!s) return rdb::Fail(RDB_E_INVALID, "rdb_server_stats_reset: null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->latencies.clear();
+  s->failed = 0;
+  s->pixels = 0;
+  s->batches = 0;
+  s->any = false;
+  s->peak = s->admitted;
   return RDB_OK;
 }
 

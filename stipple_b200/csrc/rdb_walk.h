@@ -66,20 +66,32 @@ struct BlockImage {
 // image).
 cudaError_t LaunchSourceFill(const BlockImage& im, cudaStream_t stream);
 
+// The walk's scratch is laid out for a warp: blocks are numbered across the
+// launch's images and grouped 32 at a time (group g = block / 32, lane
+// l = block % 32), and each block owns bpad positions (its length rounded up
+// to a multiple of 16; positions past the block's end hold zeros).  Position t
+// of block (g, l) sits at
+//   packed samples  32-bit word ((g * bpad/4 + t/4) * 32 + l) * 4 + t % 4
+//   float samples   float4      (g * bpad + t) * 32 + l
+//   chosen indices  byte        ((g * bpad/16 + t/16) * 32 + l) * 16 + t % 16
+// so a warp reads 4 positions of each of its 32 blocks with one 16-byte load
+// per lane (512 contiguous bytes) and writes 16 indices per lane with one
+// 16-byte store.
 struct BlockLaunch {
   const BlockImage* images;
   int n_images;
   int block;                    // positions per block (>= 16)
   int64_t total_blocks;
-  uint32_t* cx;                 // scratch: curve-ordered samples (one word per position)
-  uint8_t* chosen;              // scratch: index per curve position
-  int64_t* cx_offset;           // per image: offset of its curve positions in cx/chosen
+  uint32_t* cx;                 // scratch: samples, laid out as above
+  uint8_t* chosen;              // scratch: index per position, laid out as above
+  const int64_t* pos_offset;    // per image: its first position among all images' lists
   const unsigned char* plan;    // one palette for the launch
+  const uint32_t* cand;         // candidate table (rdb_cand.h), null with associated alpha
   int plan_smem;
   int assoc;                    // the palette associates alpha
   int is_float;                 // cx holds the sample widened to float4 (every layout but
                                 // RGB8 / RGBA8, which pack into one word)
-  int pad;
+  int bpad;                     // positions per block in the scratch (multiple of 16)
   double sw[16];
   int* status;
 };

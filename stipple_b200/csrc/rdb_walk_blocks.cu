@@ -146,29 +146,76 @@ __device__ __forceinline__ uint32_t pack_sample(const unsigned char* img, int la
          (static_cast<uint32_t>(q[2]) << 16) | 0xFF000000u;
 }
 
-// One thread per curve position of every image.
-__global__ void BlockGather(BlockLaunch L, int64_t total) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  // Images are laid out back to back in cx; find the owner by offset.
-  int lo = 0, hi = L.n_images - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (L.cx_offset[mid] <= i) lo = mid; else hi = mid - 1;
-  }
-  const BlockImage& im = L.images[lo];
-  const int64_t pos = i - L.cx_offset[lo];
-  if (pos >= im.n) return;  // alignment padding
+// The block, image and length of global block gb (the image found by binary
+// search over the images' first blocks).
+struct BlockRef {
+  const BlockImage* im;
+  int begin;  // first position of the block in its image's list
+  int len;    // positions in the block (the last block of an image may be short)
+};
+__device__ __forceinline__ BlockRef block_ref(const BlockLaunch& L, int64_t gb) {
+  const int m = find_image(L.images, L.n_images, gb);
+  const BlockImage& im = L.images[m];
+  const int b = static_cast<int>(gb - im.first_block);
+  BlockRef r;
+  r.im = &im;
+  r.begin = b * L.block;
+  r.len = min(L.block, im.n - r.begin);
+  return r;
+}
+
+// The pixel the list visits at position pos: the appended origin last.
+__device__ __forceinline__ int list_pixel(const BlockLaunch& L, const BlockImage& im, int pos) {
   int pix = (pos == im.n - 1) ? 0 : im.order[pos];
   if (static_cast<unsigned>(pix) >= static_cast<unsigned>(im.width * im.height)) {
     atomicExch(L.status, kDevBadItem);
     pix = 0;
   }
-  if (L.is_float) {
-    reinterpret_cast<float4*>(L.cx)[i] = load_wide(im, pix);
-  } else {
-    L.cx[i] = pack_sample(im.pixels, im.layout, im.row_stride, im.width, pix);
+  return pix;
+}
+
+// Packed samples: one thread per (group, 4 positions, lane), lane fastest, so
+// a warp writes 512 contiguous bytes; positions past a block's end are zero.
+__global__ void BlockGatherPacked(BlockLaunch L, int64_t quads) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= quads) return;
+  const int l = static_cast<int>(i & 31);
+  const int64_t row = i >> 5;  // g * bpad/4 + t/4
+  const int q4 = L.bpad >> 2;
+  const int64_t g = row / q4;
+  const int t0 = static_cast<int>(row - g * q4) * 4;
+  const int64_t gb = g * 32 + l;
+  uint4 w = make_uint4(0u, 0u, 0u, 0u);
+  if (gb < L.total_blocks) {
+    const BlockRef r = block_ref(L, gb);
+    uint32_t v[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (t0 + k < r.len) {
+        const int pix = list_pixel(L, *r.im, r.begin + t0 + k);
+        v[k] = pack_sample(r.im->pixels, r.im->layout, r.im->row_stride, r.im->width, pix);
+      }
+    }
+    w = make_uint4(v[0], v[1], v[2], v[3]);
   }
+  reinterpret_cast<uint4*>(L.cx)[i] = w;
+}
+
+// Widened (float4) samples: one thread per (group, position, lane).
+__global__ void BlockGatherWide(BlockLaunch L, int64_t cells) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= cells) return;
+  const int l = static_cast<int>(i & 31);
+  const int64_t row = i >> 5;  // g * bpad + t
+  const int64_t g = row / L.bpad;
+  const int t = static_cast<int>(row - g * L.bpad);
+  const int64_t gb = g * 32 + l;
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (gb < L.total_blocks) {
+    const BlockRef r = block_ref(L, gb);
+    if (t < r.len) v = load_wide(*r.im, list_pixel(L, *r.im, r.begin + t));
+  }
+  reinterpret_cast<float4*>(L.cx)[i] = v;
 }
 
 // Channel c of AssociateAlphaPixel (rd_types.h:179-192) for a packed RGBA8
@@ -219,37 +266,52 @@ __device__ __forceinline__ void RotateSums(const BlockLaunch& L, double (&R)[16]
   for (int k = 0; k < C; ++k) R[U][k] = p[k];
 }
 
-// One block: positions [begin, end) of one image's list, zeroed queue, no
-// memo.  Only the register rotation is unrolled (16 switch cases of FP64
-// work); the lookup is written once, so the loop stays in the instruction
-// cache.
+__device__ __forceinline__ uint32_t pick(const uint4& q, int k) {
+  return k == 0 ? q.x : (k == 1 ? q.y : (k == 2 ? q.z : q.w));
+}
+
+// One block of `len` positions, zeroed queue, no memo.  Only the register
+// rotation is unrolled (16 switch cases of FP64 work); the lookup is written
+// once, so the loop stays in the instruction cache.  The lookup takes the
+// key's survivors from the candidate table when the palette has one (the
+// full descent and search only for keys the table does not cover).
 template <bool kAssoc, bool kFloat>
-__device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& P, int64_t base,
-                                          int begin, int end) {
+__device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& P, int64_t g,
+                                          int lane, int len) {
   constexpr int C = kAssoc ? 4 : 3;
-  const uint32_t* cx = L.cx + base;
-  const float4* cxf = reinterpret_cast<const float4*>(L.cx) + base;
+  const uint4* cx4 = reinterpret_cast<const uint4*>(L.cx) + g * (L.bpad >> 2) * 32 + lane;
+  const float4* cxf = reinterpret_cast<const float4*>(L.cx) + g * L.bpad * 32 + lane;
+  uint4* out4 = reinterpret_cast<uint4*>(L.chosen) + g * (L.bpad >> 4) * 32 + lane;
+  const int bpad = L.bpad;
   double R[16][C];
   double e[C];
 #pragma unroll
   for (int k = 0; k < C; ++k) e[k] = 0.0;
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    double p[4] = {0.0, 0.0, 0.0, 0.0};
-    if (begin + u < end) {
-      if (kFloat) unpackf<kAssoc>(cxf[begin + u], p); else unpack8<kAssoc>(cx[begin + u], p);
-    }
+  for (int q = 0; q < 4; ++q) {
+    uint4 w = make_uint4(0u, 0u, 0u, 0u);
+    if (!kFloat) w = cx4[q * 32];
 #pragma unroll
-    for (int k = 0; k < C; ++k) R[u][k] = p[k];
+    for (int k = 0; k < 4; ++k) {
+      double p[4] = {0.0, 0.0, 0.0, 0.0};
+      if (kFloat) unpackf<kAssoc>(cxf[(4 * q + k) * 32], p); else unpack8<kAssoc>(pick(w, k), p);
+#pragma unroll
+      for (int c = 0; c < C; ++c) R[4 * q + k][c] = p[c];
+    }
   }
-  const bool word_out = ((base + begin) & 3) == 0;
-  uint32_t acc = 0;
+  uint4 ahead = make_uint4(0u, 0u, 0u, 0u);  // packed samples t+16 .. t+19
+  uint32_t acc[4] = {0u, 0u, 0u, 0u};
   int u = 0;
 #pragma unroll 1
-  for (int t = begin; t < end; ++t) {
+  for (int t = 0; t < len; ++t) {
     double p[4] = {0.0, 0.0, 0.0, 0.0};
-    if (t + 16 < end) {
-      if (kFloat) unpackf<kAssoc>(cxf[t + 16], p); else unpack8<kAssoc>(cx[t + 16], p);
+    if (t + 16 < bpad) {
+      if (kFloat) {
+        unpackf<kAssoc>(cxf[(t + 16) * 32], p);
+      } else {
+        if ((t & 3) == 0) ahead = cx4[((t + 16) >> 2) * 32];
+        unpack8<kAssoc>(pick(ahead, t & 3), p);
+      }
     }
     double v[C];
     switch (u) {
@@ -274,31 +336,40 @@ __device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& 
     float f[4];
 #pragma unroll
     for (int k = 0; k < C; ++k) f[k] = clamp_pixel(v[k]);
-    const unsigned ba = kAssoc ? byte_dev(f[C - 1]) : 0u;
-    const int node = tw::descend<kAssoc>(P, byte_dev(f[0]), byte_dev(f[1]), byte_dev(f[2]), ba);
-    double tr = f[0], tg = f[1], tb = f[2], ta = 0.0;
-    if (kAssoc) {
-      ta = f[3];
-      const double beta = __dmul_rn(kQuantumScale, ta);
-      tr = __dmul_rn(beta, tr);
-      tg = __dmul_rn(beta, tg);
-      tb = __dmul_rn(beta, tb);
+    const unsigned br = byte_dev(f[0]), bg = byte_dev(f[1]), bb = byte_dev(f[2]);
+    int index;
+    if (!kAssoc && L.cand) {
+      const uint32_t c = __ldg(L.cand + ((br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12)));
+      const unsigned s0 = c & 0xFFu, s1 = (c >> 8) & 0xFFu;
+      if (s0 == s1) {
+        index = P.seq[s0];
+      } else if (s0 < s1) {
+        index = tw::search_survivors(P, c, f[0], f[1], f[2]);
+      } else {
+        index = tw::search<false>(P, tw::descend<false>(P, br, bg, bb, 0u), f[0], f[1], f[2], 0.0);
+      }
+    } else {
+      const unsigned ba = kAssoc ? byte_dev(f[C - 1]) : 0u;
+      const int node = tw::descend<kAssoc>(P, br, bg, bb, ba);
+      double tr = f[0], tg = f[1], tb = f[2], ta = 0.0;
+      if (kAssoc) {
+        ta = f[3];
+        const double beta = __dmul_rn(kQuantumScale, ta);
+        tr = __dmul_rn(beta, tr);
+        tg = __dmul_rn(beta, tg);
+        tb = __dmul_rn(beta, tb);
+      }
+      index = tw::search<kAssoc>(P, node, tr, tg, tb, ta);
     }
-    const int index = tw::search<kAssoc>(P, node, tr, tg, tb, ta);
     const double* rc = P.rcol<kAssoc>(index);
 #pragma unroll
     for (int k = 0; k < C; ++k) e[k] = __dadd_rn(static_cast<double>(f[k]), -rc[k]);
-    if (word_out) {
-      const int q = (t - begin) & 3;
-      acc |= static_cast<uint32_t>(index) << (8 * q);
-      if (q == 3) {
-        *reinterpret_cast<uint32_t*>(L.chosen + base + t - 3) = acc;
-        acc = 0;
-      } else if (t == end - 1) {
-        for (int r = 0; r <= q; ++r) L.chosen[base + t - q + r] = static_cast<uint8_t>(acc >> (8 * r));
-      }
-    } else {
-      L.chosen[base + t] = static_cast<uint8_t>(index);
+    const int q = (t >> 2) & 3;
+    const uint32_t bits = static_cast<uint32_t>(index) << (8 * (t & 3));
+    if (q == 0) acc[0] |= bits; else if (q == 1) acc[1] |= bits; else if (q == 2) acc[2] |= bits; else acc[3] |= bits;
+    if ((t & 15) == 15 || t == len - 1) {
+      out4[(t >> 4) * 32] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+      acc[0] = acc[1] = acc[2] = acc[3] = 0u;
     }
   }
 }
@@ -315,12 +386,8 @@ __global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaun
   if (gb >= L.total_blocks) return;
   tw::Plan P;
   P.bind(smem);
-  const int im = find_image(L.images, L.n_images, gb);
-  const BlockImage& I = L.images[im];
-  const int b = static_cast<int>(gb - I.first_block);
-  const int begin = b * L.block;
-  const int end = min(begin + L.block, I.n);
-  WalkBlock<kAssoc, kFloat>(L, P, L.cx_offset[im], begin, end);
+  const BlockRef r = block_ref(L, gb);
+  WalkBlock<kAssoc, kFloat>(L, P, gb >> 5, static_cast<int>(gb & 31), r.len);
 }
 
 template <bool kAssoc, bool kFloat>
@@ -341,10 +408,10 @@ __global__ void BlockScatter(BlockLaunch L, int64_t total) {
   int lo = 0, hi = L.n_images - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (L.cx_offset[mid] <= i) lo = mid; else hi = mid - 1;
+    if (L.pos_offset[mid] <= i) lo = mid; else hi = mid - 1;
   }
   const BlockImage& im = L.images[lo];
-  const int64_t pos = i - L.cx_offset[lo];
+  const int64_t pos = i - L.pos_offset[lo];
   if (pos >= im.n) return;
   const int64_t npix = static_cast<int64_t>(im.width) * im.height;
   if (pos == 0 && im.n > 1) {
@@ -362,7 +429,10 @@ __global__ void BlockScatter(BlockLaunch L, int64_t total) {
   }
   int pix = (pos == im.n - 1) ? 0 : im.order[pos];
   if (static_cast<unsigned>(pix) >= static_cast<unsigned>(im.width * im.height)) return;
-  const uint8_t index = L.chosen[i];
+  const int64_t gb = im.first_block + pos / L.block;
+  const int64_t t = pos - (gb - im.first_block) * L.block;
+  const uint8_t index =
+      L.chosen[(((gb >> 5) * (L.bpad >> 4) + (t >> 4)) * 32 + (gb & 31)) * 16 + (t & 15)];
   if (im.indices) im.indices[pix] = index;
   if (im.rgba_out || im.raw_out) {
     // The colour as clamp_to_quantum's floats; alpha from the palette when it
@@ -411,8 +481,13 @@ cudaError_t LaunchSourceFill(const BlockImage& im, cudaStream_t stream) {
 
 cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
   if (total_positions <= 0 || L.total_blocks <= 0) return cudaSuccess;
+  const int64_t cells = (L.total_blocks + 31) / 32 * 32 * L.bpad;  // positions in the scratch
+  if (L.is_float) {
+    BlockGatherWide<<<static_cast<unsigned>((cells + 255) / 256), 256, 0, stream>>>(L, cells);
+  } else {
+    BlockGatherPacked<<<static_cast<unsigned>((cells / 4 + 255) / 256), 256, 0, stream>>>(L, cells / 4);
+  }
   const unsigned g1 = static_cast<unsigned>((total_positions + 255) / 256);
-  BlockGather<<<g1, 256, 0, stream>>>(L, total_positions);
   cudaError_t e = L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, stream) : LaunchWalk<true, false>(L, stream))
                           : (L.is_float ? LaunchWalk<false, true>(L, stream) : LaunchWalk<false, false>(L, stream));
   if (e != cudaSuccess) return e;

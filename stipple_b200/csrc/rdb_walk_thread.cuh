@@ -108,6 +108,36 @@ __device__ __forceinline__ int search(const Plan& P, int node, double tr, double
   return slot < 0 ? 0 : static_cast<int>(P.seq[slot]);
 }
 
+// ClosestColor restricted to a key's survivors (a candidate-table entry,
+// rdb_cand.h: up to four slots in ascending post-order, the last repeated):
+// the same distances in the same order with the same "<=", so the same winner.
+__device__ __forceinline__ int search_survivors(const Plan& P, uint32_t cand, double tr, double tg,
+                                                double tb) {
+  const double* dr = P.slotpal;
+  const double* dg = dr + P.slot_stride;
+  const double* db = dg + P.slot_stride;
+  double best = kSearchStart;
+  int slot = static_cast<int>(cand & 0xFFu);
+  unsigned prev = 0x100u;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const unsigned s = (cand >> (8 * i)) & 0xFFu;
+    if (s == prev) break;
+    prev = s;
+    const double x = __dadd_rn(dr[s], -tr);
+    const double y = __dadd_rn(dg[s], -tg);
+    const double z = __dadd_rn(db[s], -tb);
+    double d = __dmul_rn(x, x);
+    d = __dadd_rn(d, __dmul_rn(y, y));
+    d = __dadd_rn(d, __dmul_rn(z, z));
+    if (d <= best) {
+      best = d;
+      slot = static_cast<int>(s);
+    }
+  }
+  return static_cast<int>(P.seq[slot]);
+}
+
 // The same search spread over the 32 lanes of a warp for ONE target (every
 // lane passes the same node and target): lane l scans slots start+l,
 // start+l+32, ..., keeping its last minimum; the butterfly then keeps the

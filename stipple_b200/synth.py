@@ -74,6 +74,35 @@ def video_frame(width: int, height: int, seed: int, frame: int, sigma: float = 6
                          noise_seed=seed * 100003 + frame + 1)
 
 
+def video_clip_device(width: int, height: int, seed: int, frames: int, device="cuda",
+                      sigma: float = 6.0, px_per_frame: float = 2.0):
+    """The video clip of video_frame (same seeded gradients, translating
+    px_per_frame pixels a frame), generated on the device as a torch uint8
+    tensor (frames, H, W, 3).  The per-frame Gaussian noise is drawn from
+    torch's generator seeded per frame, so the frames differ from
+    video_frame's in the noise draw only; used where a long clip is needed
+    fast (120 4K frames), parity tests use video_frame."""
+    import torch
+    rng = np.random.default_rng(seed)
+    waves = _waves(rng, 3)
+    n = float(max(width, height, 1))
+    out = torch.empty((frames, height, width, 3), dtype=torch.uint8, device=device)
+    ys = torch.arange(height, dtype=torch.float64, device=device)[:, None]
+    gen = torch.Generator(device=device)
+    for f in range(frames):
+        xs = (torch.arange(width, dtype=torch.float64, device=device) - px_per_frame * f)[None, :]
+        gen.manual_seed(seed * 100003 + f + 1)
+        for c in range(3):
+            acc = torch.full((height, width), 128.0, dtype=torch.float64, device=device)
+            for amp, phase, fx, fy in waves[c]:
+                acc += amp * torch.sin(2.0 * math.pi * (fx * xs + fy * ys) / n + phase)
+            if sigma > 0:
+                acc += sigma * torch.randn((height, width), dtype=torch.float64, device=device,
+                                           generator=gen)
+            out[f, :, :, c] = torch.clamp(torch.round(acc), 0, 255).to(torch.uint8)
+    return out
+
+
 def to_q16(img8: np.ndarray) -> np.ndarray:
     """uint8 (H, W, 3|4) -> float32 (H, W, 4) Q16 RGBA, opaque when no alpha."""
     h, w, c = img8.shape
@@ -94,6 +123,18 @@ def log_uniform_sizes(n: int, seed: int, lo: int = 1, hi: int = 4096):
     ws = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(int)
     hs = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(int)
     return [(int(max(lo, w)), int(max(lo, h))) for w, h in zip(ws, hs)]
+
+
+def mixed_batch_spec(n: int = 512, seed: int = 2024):
+    """The mixed-size batch of uneven RGBA8 images: n - 4 sizes with W and H
+    each log-uniform in 1..4096, plus the forced 1x1, 3x5, 17x13 and 4096x64
+    strips.  Returns [(width, height, image_seed, colours)], colours drawn
+    from {2, 4, 8, 16, 64, 256}; image k is gradient_rgba8(w, h, image_seed)
+    (about 20 % transparent) and gets its own alpha-associated palette."""
+    sizes = log_uniform_sizes(n - 4, seed=seed) + [(1, 1), (3, 5), (17, 13), (4096, 64)]
+    rng = np.random.default_rng(5)
+    return [(w, h, 1000 + k, int(rng.choice([2, 4, 8, 16, 64, 256])))
+            for k, (w, h) in enumerate(sizes)]
 
 
 # ---- decoder-format video frames --------------------------------------------

@@ -78,7 +78,7 @@ def test_reader_rules(sb, tmp_path):
     p.write_text("# nothing\n")
     with pytest.raises(sb.RdbError, match="no palette rows"):
         sb.read_palette_text(str(p))
-    with pytest.raises(sb.RdbError, match="PNG8"):
+    with pytest.raises(sb.RdbError, match="rdb_palette_read_png"):
         sb.read_palette_text(str(tmp_path / "pal.png"))
-    with pytest.raises(sb.RdbError, match="PNG8"):
+    with pytest.raises(sb.RdbError, match="rdb_palette_write_png"):
         sb.write_palette_text(np.zeros((2, 4)), str(tmp_path / "pal.png"))
