@@ -138,6 +138,15 @@ typedef struct rdb_kernel_stats {
   int64_t chains;          /* segments (concurrent chains) of the last segmented walk */
 } rdb_kernel_stats;
 int rdb_context_profile(rdb_context* ctx, int enable);
+/* The block engine's index dump, the reference's `<prefix>.idx.bin`
+ * (src/rd_opencl.cpp:2137-2147, written when RD_OCL_DUMP names a prefix):
+ * while `prefix` is set, every block-engine call of the context (rdb_dither
+ * with RDB_ENGINE_BLOCKS, rdb_dither_frames*) writes `<prefix>.idx.bin`, the
+ * palette index chosen at every position of every image's block-mode list
+ * (src/rd_riemersma_cpu.cpp:269-356), one byte each, in list order, images in
+ * call order, replacing the file of the previous call.  The call then waits
+ * for the device.  NULL or "" turns it off. */
+int rdb_context_dump_indices(rdb_context* ctx, const char* prefix);
 int rdb_context_stats(const rdb_context* ctx, rdb_kernel_stats* out);
 
 /* Dependent latency in SM cycles of each operation on the sequential walk's

@@ -577,19 +577,11 @@ void orc_walk_seq(const orc_tree* t, const orc_entry* palette, int count,
   free(cache);
 }
 
-/* src/rd_riemersma_cpu.cpp:477-805 (RiemersmaBlocksCpu), RgbaF path, 1 frame. */
-int orc_walk_blocks(const orc_tree* t, const orc_entry* palette, int count,
-                    int assoc, double diffusion, int block, size_t width,
-                    size_t height, float* pixels, uint8_t* idx_out) {
-  if (count > 256) return -1;
-  if (block < QUEUE) return -1;
-  double sw[16];
-  scaled_weights(diffusion, sw);
-  const size_t pixels_n = width * height;
-  int32_t* curve = (int32_t*)malloc((pixels_n + 1) * sizeof(int32_t));
-  int32_t* owner = (int32_t*)malloc((pixels_n ? pixels_n : 1) * sizeof(int32_t));
-  const int n = (int)orc_block_order(width, height, curve, owner);
-  uint8_t* chosen = (uint8_t*)malloc((size_t)(n > 0 ? n : 1));
+/* The walk of RiemersmaBlocksCpu (src/rd_riemersma_cpu.cpp:640-696): every
+ * block of the list from a zeroed queue, no memo; chosen[i] per position. */
+static void block_walk_chosen(const orc_tree* t, const orc_entry* palette, int assoc,
+                              const double sw[16], int block, const int32_t* curve, int n,
+                              const float* pixels, uint8_t* chosen) {
   const int nblocks = (n + block - 1) / block;
   for (int b = 0; b < nblocks; ++b) {
     dpix err[16];
@@ -619,6 +611,22 @@ int orc_walk_blocks(const orc_tree* t, const orc_entry* palette, int count,
       if (assoc) err[QUEUE - 1].a = pixel.a - color.a;
     }
   }
+}
+
+/* src/rd_riemersma_cpu.cpp:477-805 (RiemersmaBlocksCpu), RgbaF path, 1 frame. */
+int orc_walk_blocks(const orc_tree* t, const orc_entry* palette, int count,
+                    int assoc, double diffusion, int block, size_t width,
+                    size_t height, float* pixels, uint8_t* idx_out) {
+  if (count > 256) return -1;
+  if (block < QUEUE) return -1;
+  double sw[16];
+  scaled_weights(diffusion, sw);
+  const size_t pixels_n = width * height;
+  int32_t* curve = (int32_t*)malloc((pixels_n + 1) * sizeof(int32_t));
+  int32_t* owner = (int32_t*)malloc((pixels_n ? pixels_n : 1) * sizeof(int32_t));
+  const int n = (int)orc_block_order(width, height, curve, owner);
+  uint8_t* chosen = (uint8_t*)malloc((size_t)(n > 0 ? n : 1));
+  block_walk_chosen(t, palette, assoc, sw, block, curve, n, pixels, chosen);
   for (int i = 0; i < n; ++i) {
     const int p = curve[i];
     if (owner[p] != i) continue;
@@ -634,6 +642,26 @@ int orc_walk_blocks(const orc_tree* t, const orc_entry* palette, int count,
   free(owner);
   free(curve);
   return 0;
+}
+
+/* The chosen index at every position of the block-mode list, in list order
+ * (the array src/rd_riemersma_cpu.cpp:640-696 fills before its owner
+ * scatter).  Returns the list length, or -1 for the refusals. */
+int orc_block_chosen(const orc_tree* t, const orc_entry* palette, int count, int assoc,
+                     double diffusion, int block, size_t width, size_t height,
+                     const float* pixels, uint8_t* chosen_out) {
+  if (count > 256) return -1;
+  if (block < QUEUE) return -1;
+  double sw[16];
+  scaled_weights(diffusion, sw);
+  const size_t pixels_n = width * height;
+  int32_t* curve = (int32_t*)malloc((pixels_n + 1) * sizeof(int32_t));
+  int32_t* owner = (int32_t*)malloc((pixels_n ? pixels_n : 1) * sizeof(int32_t));
+  const int n = (int)orc_block_order(width, height, curve, owner);
+  block_walk_chosen(t, palette, assoc, sw, block, curve, n, pixels, chosen_out);
+  free(owner);
+  free(curve);
+  return n;
 }
 
 /* src/rd_approx_cuda.cu:73-88 (BuildInverseFilter) */

@@ -96,6 +96,13 @@ int orc_walk_blocks(const orc_tree* t, const orc_entry* palette, int count,
                     int associate_alpha, double diffusion, int block,
                     size_t width, size_t height, float* pixels, uint8_t* idx_out);
 
+/* The chosen index at every block-list position, in list order (the buffer
+ * the reference's block engines dump as `.idx.bin`).  chosen_out holds
+ * W*H+1 bytes; returns the list length or -1 for the refusals. */
+int orc_block_chosen(const orc_tree* t, const orc_entry* palette, int count, int assoc,
+                     double diffusion, int block, size_t width, size_t height,
+                     const float* pixels, uint8_t* chosen_out);
+
 /* Video frame formats (codes as the library's RDB_* formats: 3 RGB8, 4 RGBA8,
  * 16 RgbaF, 6 rgb48, 8 rgba64, 444 planar 4:4:4, 420 planar 4:2:0).
  * orc_widen_frame: src/rd_riemersma_cpu.cpp:496-516 (gather_pixel),

@@ -92,6 +92,9 @@ class Oracle:
         lib.orc_walk_blocks.argtypes = [C.POINTER(OrcTree), _f64p, C.c_int, C.c_int, C.c_double,
                                         C.c_int, C.c_size_t, C.c_size_t, _f32p, _u8p]
         lib.orc_walk_blocks.restype = C.c_int
+        lib.orc_block_chosen.argtypes = [C.POINTER(OrcTree), _f64p, C.c_int, C.c_int, C.c_double,
+                                         C.c_int, C.c_size_t, C.c_size_t, _f32p, _u8p]
+        lib.orc_block_chosen.restype = C.c_int
         lib.orc_seq_order.argtypes = [C.c_size_t, C.c_size_t, _i32p]
         lib.orc_seq_order.restype = C.c_size_t
         lib.orc_block_order.argtypes = [C.c_size_t, C.c_size_t, _i32p, _i32p]
@@ -187,6 +190,29 @@ class Oracle:
             if rc != 0:
                 raise ValueError("blocks walk refused")
             return idx.reshape(h, w), out.reshape(h, w, 4), pal.reshape(-1, 4)[:count]
+        finally:
+            self.lib.orc_tree_free(C.byref(t))
+
+    def block_chosen(self, rgbaf: np.ndarray, max_colors: int, assoc: bool, gray: bool,
+                     block: int, diffusion: float = 1.0) -> np.ndarray:
+        """The chosen index at every block-list position (list order)."""
+        return self.block_chosen_with_tree(rgbaf, rgbaf, max_colors, assoc, gray, block, diffusion)
+
+    def block_chosen_with_tree(self, tree_src: np.ndarray, rgbaf: np.ndarray, max_colors: int,
+                               assoc: bool, gray: bool, block: int,
+                               diffusion: float = 1.0) -> np.ndarray:
+        """block_chosen of `rgbaf` with the tree built from `tree_src`."""
+        h, w = rgbaf.shape[:2]
+        t = self.build_tree_raw(tree_src, max_colors, assoc, gray)
+        try:
+            pal = np.ctypeslib.as_array(t.colormap, shape=(max(t.color_count, 1) * 4,)).copy()
+            px = np.ascontiguousarray(rgbaf, dtype=np.float32).reshape(-1)
+            out = np.zeros(w * h + 1, np.uint8)
+            n = self.lib.orc_block_chosen(C.byref(t), pal, t.color_count, int(assoc),
+                                          float(diffusion), int(block), w, h, px, out)
+            if n < 0:
+                raise ValueError("blocks walk refused")
+            return out[:n]
         finally:
             self.lib.orc_tree_free(C.byref(t))
 

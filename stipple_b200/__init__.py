@@ -176,6 +176,7 @@ SIGNATURES = {
     "rdb_server_stats_get": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rdb_server_stats_reset": (C.c_int, [C.c_void_p]),
     "rdb_probe_latency": (C.c_int, [C.c_int, C.c_void_p]),
+    "rdb_context_dump_indices": (C.c_int, [C.c_void_p, C.c_char_p]),
     "rdb_palette_write_png": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
     "rdb_palette_read_png": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "rdb_server_destroy": (None, [C.c_void_p]),
@@ -332,6 +333,10 @@ class Context:
     def last_passes(self) -> int:
         """Passes the last segmented sequential walk took."""
         return load().rdb_context_last_passes(self.handle)
+
+    def dump_indices(self, prefix: str | None) -> None:
+        """rdb_context_dump_indices: block walks write `<prefix>.idx.bin`."""
+        _check(load().rdb_context_dump_indices(self.handle, (prefix or "").encode()))
 
     def profile(self, enable: bool = True) -> None:
         """Turns the walk-kernel counters on or off (and clears them)."""

@@ -239,6 +239,12 @@ int rdb_context_profile(rdb_context* ctx, int enable) {
   return ctx->impl.Profile(enable != 0);
 }
 
+int rdb_context_dump_indices(rdb_context* ctx, const char* prefix) {
+  if (!ctx) return Guard("rdb_context_dump_indices");
+  ctx->impl.DumpIndices(prefix ? prefix : "");
+  return RDB_OK;
+}
+
 int rdb_context_stats(const rdb_context* ctx, rdb_kernel_stats* out) {
   if (!ctx || !out) return Guard("rdb_context_stats");
   *out = ctx->impl.stats();

@@ -7,6 +7,8 @@
 // the glibc qsort with a tolerance comparator for the reduction threshold.
 #include "rdb_octree.h"
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -15,8 +17,6 @@
 
 namespace rdb {
 namespace {
-
-constexpr std::size_t kMaxQNodes = 266817;  // quantize.c MaxQNodes (rd_octree.h:39)
 
 // rd_octree.cpp:23-29: returns 0 for values within 1e-12, so the sort is
 // deterministic only for this exact comparator and qsort implementation.
@@ -217,9 +217,7 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
   }
 }
 
-void Octree::Build(const void* pixels, PixelLayout layout, std::size_t width,
-                   std::size_t height, std::size_t row_stride_bytes, int max_colors,
-                   bool associate_alpha, bool grayscale) {
+void Octree::Setup(int max_colors, bool associate_alpha, bool grayscale) {
   nodes_.clear();
   colormap_.clear();
   assoc_ = associate_alpha;
@@ -244,44 +242,9 @@ void Octree::Build(const void* pixels, PixelLayout layout, std::size_t width,
   Add(0, 0, -1);
   live_ = 1;
   nodes_[0].parent = 0;  // GetQCubeInfo's root->parent = root (rd_octree.cpp:285)
+}
 
-  // Rows are widened to Q16 floats one at a time.
-  std::vector<float> widened(width * 4);
-  const auto row_at = [&](std::size_t y) -> const float* {
-    const unsigned char* base = static_cast<const unsigned char*>(pixels) + y * row_stride_bytes;
-    if (layout == PixelLayout::kRgbaF32) return reinterpret_cast<const float*>(base);
-    const int ch = static_cast<int>(layout);
-    for (std::size_t x = 0; x < width; ++x) {
-      widened[4 * x + 0] = static_cast<float>(base[ch * x + 0]) * 257.0f;
-      widened[4 * x + 1] = static_cast<float>(base[ch * x + 1]) * 257.0f;
-      widened[4 * x + 2] = static_cast<float>(base[ch * x + 2]) * 257.0f;
-      widened[4 * x + 3] = ch == 4 ? static_cast<float>(base[ch * x + 3]) * 257.0f : 65535.0f;
-    }
-    return widened.data();
-  };
-
-  // rd_octree.cpp:364-385: the two classification loops with different limits.
-  std::size_t y = 0;
-  for (; y < height; ++y) {
-    if (live_ > kMaxQNodes) {
-      PruneAtDepth(0);
-      --depth_;
-    }
-    Classify(row_at(y), width, kMaxTreeDepth, kMaxTreeDepth);
-    if (colors_ > max_colors_) {
-      PruneBelowDepth(0);
-      break;
-    }
-  }
-  ++y;
-  for (; y < height; ++y) {
-    if (live_ > kMaxQNodes) {
-      PruneAtDepth(0);
-      --depth_;
-    }
-    Classify(row_at(y), width, depth_, depth_);
-  }
-
+void Octree::Finish() {
   // rd_octree.cpp:387-404 (ReduceImageColors).
   if (colors_ > max_colors_) {
     next_prune_ = 0.0;
@@ -302,6 +265,105 @@ void Octree::Build(const void* pixels, PixelLayout layout, std::size_t width,
     ReducePass(0);
   }
   Colormap(0);
+}
+
+void Octree::KeysBelow(int32_t node, uint32_t path, std::vector<uint64_t>* keys,
+                       std::vector<int32_t>* index) const {
+  const int bits = assoc_ ? 4 : 3;
+  for (int i = 0; i < Fan(); ++i) {
+    const int32_t c = nodes_[node].child[i];
+    if (c < 0) continue;
+    const uint32_t p = (path << bits) | static_cast<uint32_t>(i);
+    keys->push_back(NodeKey(static_cast<int>(nodes_[c].level), p));
+    index->push_back(c);
+    KeysBelow(c, p, keys, index);
+  }
+}
+
+void Octree::LiveKeys(std::vector<uint64_t>* keys, std::vector<int32_t>* index) const {
+  keys->clear();
+  index->clear();
+  KeysBelow(0, 0u, keys, index);
+}
+
+bool Octree::Absorb(const OctreeRows& r) {
+  const int bits = assoc_ ? 4 : 3;
+  // The root accumulates every visited node's running error; its exact bits
+  // decide nothing as long as it exceeds every other node's error by more than
+  // the reduction's one-unit step (it then sorts last, is never merged and
+  // never becomes the next threshold), so a sum in another order stands in.
+  double max_other = 0.0;
+  for (const OctNode& n : nodes_) max_other = std::max(max_other, n.qerr);
+  for (double q : r.qerr) max_other = std::max(max_other, q);
+  const double root = nodes_[0].qerr + r.root_gain;
+  if (!(root > max_other * (1.0 + 1e-9) + 2.0)) return false;
+  if (live_ + r.keys.size() > kMaxNodes) return false;  // the loop would have pruned
+  std::vector<uint64_t> keys;
+  std::vector<int32_t> index;
+  LiveKeys(&keys, &index);
+  // Existing nodes by key (sorted for lookup).
+  std::vector<std::pair<uint64_t, int32_t>> have(keys.size());
+  for (std::size_t i = 0; i < keys.size(); ++i) have[i] = {keys[i], index[i]};
+  std::sort(have.begin(), have.end());
+  const auto find = [&](uint64_t k) -> int32_t {
+    auto it = std::lower_bound(have.begin(), have.end(), std::make_pair(k, INT32_MIN));
+    return (it != have.end() && it->first == k) ? it->second : -1;
+  };
+  // Keys ascend by level, so every parent exists before its children.
+  std::vector<std::pair<uint64_t, int32_t>> made;
+  const auto node_of = [&](uint64_t k) -> int32_t {
+    const int32_t n = find(k);
+    if (n >= 0) return n;
+    auto it = std::lower_bound(made.begin(), made.end(), std::make_pair(k, INT32_MIN));
+    return (it != made.end() && it->first == k) ? it->second : -1;
+  };
+  for (std::size_t i = 0; i < r.keys.size(); ++i) {
+    const uint64_t k = r.keys[i];
+    const int level = static_cast<int>(k >> 32);
+    const uint32_t path = static_cast<uint32_t>(k);
+    int32_t node = node_of(k);
+    if (node < 0) {
+      const int32_t parent = level == 1 ? 0 : node_of(NodeKey(level - 1, path >> bits));
+      if (parent < 0) return false;
+      const uint32_t id = path & ((1u << bits) - 1u);
+      node = Add(id, static_cast<uint32_t>(level), parent);
+      nodes_[parent].child[id] = node;
+      ++live_;
+      if (level == depth_) ++colors_;
+      made.insert(std::upper_bound(made.begin(), made.end(), std::make_pair(k, node)), {k, node});
+    }
+    nodes_[node].qerr = r.qerr[i];
+  }
+  for (std::size_t i = 0; i < r.leaf_keys.size(); ++i) {
+    const int32_t node = node_of(r.leaf_keys[i]);
+    if (node < 0) return false;
+    nodes_[node].number_unique = r.leaf_count[i];
+    for (int c = 0; c < 4; ++c) nodes_[node].total[c] = r.leaf_total[4 * i + c];
+  }
+  nodes_[0].qerr = root;
+  return true;
+}
+
+void Octree::Build(const void* pixels, PixelLayout layout, std::size_t width,
+                   std::size_t height, std::size_t row_stride_bytes, int max_colors,
+                   bool associate_alpha, bool grayscale) {
+  // Rows are widened to Q16 floats one at a time.
+  std::vector<float> widened(width * 4);
+  const auto row_at = [&](std::size_t y) -> const float* {
+    const unsigned char* base = static_cast<const unsigned char*>(pixels) + y * row_stride_bytes;
+    if (layout == PixelLayout::kRgbaF32) return reinterpret_cast<const float*>(base);
+    const int ch = static_cast<int>(layout);
+    for (std::size_t x = 0; x < width; ++x) {
+      widened[4 * x + 0] = static_cast<float>(base[ch * x + 0]) * 257.0f;
+      widened[4 * x + 1] = static_cast<float>(base[ch * x + 1]) * 257.0f;
+      widened[4 * x + 2] = static_cast<float>(base[ch * x + 2]) * 257.0f;
+      widened[4 * x + 3] = ch == 4 ? static_cast<float>(base[ch * x + 3]) * 257.0f : 65535.0f;
+    }
+    return widened.data();
+  };
+  const std::size_t y0 = Begin(row_at, width, height, max_colors, associate_alpha, grayscale);
+  ClassifyRows(row_at, width, y0, height);
+  Finish();
 }
 
 void error_weights(double w[kQueue]) {

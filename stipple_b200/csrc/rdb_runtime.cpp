@@ -2,6 +2,7 @@
 #include "rdb_runtime.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <map>
 #include <tuple>
 #include <mutex>
@@ -643,6 +644,25 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
   L.status = static_cast<int*>(status_.ptr);
   e = LaunchBlockWalk(L, positions, s);
   if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
+  if (!dump_prefix_.empty()) return DumpBlockIndices(L, positions, s);
+  return RDB_OK;
+}
+
+// The reference's `.idx.bin` debug dump (src/rd_opencl.cpp:2137-2147): the
+// walk's index buffer as raw bytes, one per list position.  Synchronous.
+int Context::DumpBlockIndices(const BlockLaunch& L, int64_t positions, cudaStream_t s) {
+  if (int rc = Reserve(&dump_buf_, static_cast<std::size_t>(positions), "index dump")) return rc;
+  uint8_t* d = static_cast<uint8_t*>(dump_buf_.ptr);
+  std::vector<uint8_t> host(static_cast<std::size_t>(positions));
+  cudaError_t e = LaunchBlockChosenLinear(L, positions, d, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), d, host.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return CudaFail(e, "index dump");
+  const std::string path = dump_prefix_ + ".idx.bin";
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) return Fail(RDB_E_INVALID, "cannot open " + path + " for writing");
+  const bool ok = std::fwrite(host.data(), 1, host.size(), f) == host.size();
+  if (std::fclose(f) != 0 || !ok) return Fail(RDB_E_INVALID, "cannot write " + path);
   return RDB_OK;
 }
 

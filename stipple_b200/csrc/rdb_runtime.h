@@ -83,6 +83,7 @@ class Context {
   // The palette's candidate table (rdb_cand.h); palettes without associated
   // alpha only.
   int Candidates(int id, cudaStream_t s, const uint32_t** out);
+  int DumpBlockIndices(const BlockLaunch& L, int64_t positions, cudaStream_t s);
 
   // Visit order of a geometry, built on first use and kept resident.
   int Order(int width, int height, cudaStream_t s, const int32_t** out);
@@ -174,6 +175,8 @@ class Context {
   DevBuf tsw_g_;
   int last_passes_ = 0;
   bool profiling_ = false;
+  std::string dump_prefix_;   // rdb_context_dump_indices: "" = off
+  DevBuf dump_buf_;
   rdb_kernel_stats stats_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};
   // Pipelined pass loop of the segmented walk: a pinned ring of per-pass
@@ -200,6 +203,9 @@ class Context {
   // for that call's stream and reads the loop's own count.
   int last_passes();
   int Profile(bool on);
+  // Block walks write `<prefix>.idx.bin` (every image's chosen index at every
+  // block-list position, in list order, images in call order); "" = off.
+  void DumpIndices(const std::string& prefix) { dump_prefix_ = prefix; }
   const rdb_kernel_stats& stats() const { return stats_; }
 };
 

@@ -97,6 +97,10 @@ struct BlockLaunch {
 };
 
 cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream);
+// The chosen index of every position of every image, in list order, images
+// back to back (`out`: total_positions bytes).
+cudaError_t LaunchBlockChosenLinear(const BlockLaunch& L, int64_t total_positions, uint8_t* out,
+                                    cudaStream_t stream);
 
 // Writes every pixel's source value, as RgbaF, into `out` -- the result an
 // engine that visits nothing leaves (a 1x1 image in block mode).

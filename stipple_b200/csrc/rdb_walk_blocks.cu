@@ -445,6 +445,21 @@ __global__ void BlockScatter(BlockLaunch L, int64_t total) {
   }
 }
 
+__global__ void ChosenLinear(BlockLaunch L, int64_t total, uint8_t* out) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int lo = 0, hi = L.n_images - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L.pos_offset[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  const BlockImage& im = L.images[lo];
+  const int64_t pos = i - L.pos_offset[lo];
+  const int64_t gb = im.first_block + pos / L.block;
+  const int64_t t = pos - (gb - im.first_block) * L.block;
+  out[i] = L.chosen[(((gb >> 5) * (L.bpad >> 4) + (t >> 4)) * 32 + (gb & 31)) * 16 + (t & 15)];
+}
+
 __global__ void SourceFill(BlockImage im) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= static_cast<int64_t>(im.width) * im.height) return;
@@ -476,6 +491,14 @@ cudaError_t LaunchSourceFill(const BlockImage& im, cudaStream_t stream) {
   const int64_t n = static_cast<int64_t>(im.width) * im.height;
   if (n <= 0 || (!im.rgba_out && !im.raw_out)) return cudaSuccess;
   SourceFill<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(im);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchBlockChosenLinear(const BlockLaunch& L, int64_t total_positions, uint8_t* out,
+                                    cudaStream_t stream) {
+  if (total_positions <= 0) return cudaSuccess;
+  ChosenLinear<<<static_cast<unsigned>((total_positions + 255) / 256), 256, 0, stream>>>(
+      L, total_positions, out);
   return cudaGetLastError();
 }
 

@@ -116,3 +116,29 @@ def oracle_blocks_with_tree(oracle, palette_src, img, colors, block):
         return idx.reshape(h, w)
     finally:
         oracle.lib.orc_tree_free(C.byref(raw))
+
+
+@pytest.mark.parametrize("w,h,colors,block,alpha", [(256, 192, 64, 37, False), (100, 37, 16, 256, False),
+                                                     (64, 48, 8, 16, True)])
+def test_idx_bin_dump(ctx, oracle, tmp_path, w, h, colors, block, alpha):
+    """rdb_context_dump_indices: the chosen index at every block-list position,
+    list order, images in call order -- the reference's `.idx.bin`."""
+    imgs = [(synth.gradient_rgba8 if alpha else synth.gradient_rgb8)(w, h, s) for s in (5, 6)]
+    t = sb.Octree(imgs[0], colors, alpha)
+    pid = ctx.palette_from_octree(t)
+    prefix = str(tmp_path / "dump")
+    ctx.dump_indices(prefix)
+    try:
+        ctx.dither_host("blocks", imgs, [pid, pid], block=block)
+    finally:
+        ctx.dump_indices(None)
+        ctx.release_palette(pid)
+    got = np.fromfile(prefix + ".idx.bin", np.uint8)
+    # The oracle builds its tree from the image it walks: walk each image with
+    # the first image's tree by building from the first and checking both
+    # images' lists in order.
+    want = []
+    for img in imgs:
+        want.append(oracle.block_chosen_with_tree(synth.to_q16(imgs[0]), synth.to_q16(img), colors,
+                                                  alpha, t.grayscale, block))
+    assert np.array_equal(got, np.concatenate(want))
