@@ -62,9 +62,24 @@ int rdb_max_frames(int device, int engine, size_t width, size_t height, size_t v
  * octree classification, reduction to at most `max_colors` and colormap, on
  * the host.  `row_stride` is in bytes (0 = packed). */
 typedef struct rdb_octree rdb_octree;
+typedef struct rdb_context rdb_context;
 int rdb_octree_build(const void* pixels, int layout, size_t width, size_t height,
                      size_t row_stride, int max_colors, int associate_alpha, int grayscale,
                      rdb_octree** out);
+/* The same build of an image in DEVICE memory (ctx's device), its rows after
+ * the build's first loop classified on the device: each run of equal pixels
+ * adds to one node per level, contributions are computed in parallel and each
+ * node's are added in the reference's row-major order by one thread, so every
+ * node's error, count and totals -- the tree and the colormap -- are those of
+ * rdb_octree_build.  The root's accumulated error, which decides nothing once
+ * it exceeds every other node's, is summed in another order (checked; when it
+ * does not exceed them the rows are classified on the host instead).  The
+ * node array lists the live nodes in another order than rdb_octree_build's
+ * (and without the pruned ones).  Synchronous on `stream`.  *device_rows (may
+ * be NULL) receives how many rows the device classified. */
+int rdb_octree_build_device(rdb_context* ctx, const void* pixels, int layout, size_t width,
+                            size_t height, size_t row_stride, int max_colors, int associate_alpha,
+                            int grayscale, void* stream, rdb_octree** out, int* device_rows);
 int rdb_octree_color_count(const rdb_octree* t);
 int rdb_octree_node_count(const rdb_octree* t);
 int rdb_octree_depth(const rdb_octree* t);
@@ -113,7 +128,6 @@ int rdb_is_grayscale(const void* pixels, int layout, size_t width, size_t height
  * geometry, memo slabs and scratch.  The reference keeps comparable state in
  * its blocks engine's DeviceState slots (src/rd_blocks_cuda.cu:855-1002).
  * A context is used by one host thread at a time. */
-typedef struct rdb_context rdb_context;
 /* memory_budget: bytes of device memory the context may hold (0 = 90 % of free). */
 int rdb_context_create(int device, size_t memory_budget, rdb_context** out);
 void rdb_context_destroy(rdb_context* ctx);

@@ -177,6 +177,9 @@ SIGNATURES = {
     "rdb_server_stats_reset": (C.c_int, [C.c_void_p]),
     "rdb_probe_latency": (C.c_int, [C.c_int, C.c_void_p]),
     "rdb_context_dump_indices": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "rdb_octree_build_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_size_t, C.c_size_t,
+                                          C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                          C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
     "rdb_palette_write_png": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
     "rdb_palette_read_png": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "rdb_server_destroy": (None, [C.c_void_p]),
@@ -348,6 +351,21 @@ class Context:
         return {f: getattr(st, f) for f, _ in KernelStats._fields_}
 
     # -- palettes ---------------------------------------------------------
+    def octree_device(self, pixels: int, layout: int, width: int, height: int, max_colors: int,
+                      associate_alpha: bool = False, grayscale: bool = False, row_stride: int = 0,
+                      stream: int | None = None) -> tuple[Octree, int]:
+        """rdb_octree_build_device: the palette build of an image in device
+        memory (`pixels` a device pointer).  Returns the tree and how many rows
+        the device classified."""
+        t = Octree(None)
+        rows = C.c_int(0)
+        _check(load().rdb_octree_build_device(self.handle, pixels, layout, width, height, row_stride,
+                                              int(max_colors), int(associate_alpha), int(grayscale),
+                                              stream or None, C.byref(t.handle), C.byref(rows)))
+        t.associate_alpha = bool(associate_alpha)
+        t.grayscale = bool(grayscale)
+        return t, rows.value
+
     def palette_from_octree(self, tree: Octree) -> int:
         pid = C.c_int()
         _check(load().rdb_palette_from_octree(self.handle, tree.handle, C.byref(pid)))

@@ -48,6 +48,7 @@ SOURCES = [
     "rdb_uniform.cu",
     "rdb_probe.cu",
     "rdb_cand.cu",
+    "rdb_octree_dev.cu",
 ]
 
 

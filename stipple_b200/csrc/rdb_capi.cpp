@@ -112,6 +112,32 @@ int rdb_octree_build(const void* pixels, int layout, size_t width, size_t height
   return RDB_OK;
 }
 
+int rdb_octree_build_device(rdb_context* ctx, const void* pixels, int layout, size_t width,
+                            size_t height, size_t row_stride, int max_colors, int associate_alpha,
+                            int grayscale, void* stream, rdb_octree** out, int* device_rows) {
+  if (!ctx || !pixels || !out) return Guard("rdb_octree_build_device");
+  *out = nullptr;
+  if (!LayoutOk(layout)) return rdb::Fail(RDB_E_INVALID, "unknown pixel layout");
+  if (width == 0 || height == 0) return rdb::Fail(RDB_E_INVALID, "empty image");
+  if (width * height >= (std::size_t{1} << 31) / 8) {
+    return rdb::Fail(RDB_E_UNSUPPORTED, "rdb_octree_build_device takes images below 2^28 pixels");
+  }
+  rdb_octree* t = new (std::nothrow) rdb_octree();
+  if (!t) return rdb::Fail(RDB_E_NOMEM, "octree allocation");
+  const std::size_t stride = row_stride ? row_stride : width * LayoutBytes(layout);
+  int rows = 0;
+  const int rc = ctx->impl.BuildOctree(pixels, layout, static_cast<int>(width), static_cast<int>(height),
+                                       stride, max_colors, associate_alpha != 0, grayscale != 0,
+                                       static_cast<cudaStream_t>(stream), &t->tree, &rows);
+  if (rc != RDB_OK) {
+    delete t;
+    return rc;
+  }
+  if (device_rows) *device_rows = rows;
+  *out = t;
+  return RDB_OK;
+}
+
 int rdb_octree_color_count(const rdb_octree* t) { return t ? t->tree.color_count() : 0; }
 int rdb_octree_node_count(const rdb_octree* t) {
   return t ? static_cast<int>(t->tree.nodes().size()) : 0;

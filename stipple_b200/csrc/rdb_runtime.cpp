@@ -14,6 +14,7 @@
 #include "rdb_ssw.h"
 #include "rdb_tsw.h"
 #include "rdb_cand.h"
+#include "rdb_octree_dev.h"
 #include "rdb_uniform.h"
 
 namespace rdb {
@@ -645,6 +646,101 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
   e = LaunchBlockWalk(L, positions, s);
   if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
   if (!dump_prefix_.empty()) return DumpBlockIndices(L, positions, s);
+  return RDB_OK;
+}
+
+int Context::BuildOctree(const void* pixels, int layout, int width, int height, std::size_t stride,
+                         int max_colors, bool assoc, bool gray, cudaStream_t s, Octree* out,
+                         int* device_rows) {
+  if (!s) s = stream_;
+  cudaSetDevice(device_);
+  *device_rows = 0;
+  const std::size_t W = static_cast<std::size_t>(width);
+  const std::size_t bpp = layout == RDB_RGBAF32 ? 16 : static_cast<std::size_t>(layout);
+  // Rows for the host loops, copied back one at a time and widened to Q16.
+  std::vector<unsigned char> raw(W * bpp);
+  std::vector<float> widened(W * 4);
+  cudaError_t fetch_error = cudaSuccess;
+  const auto row_at = [&](std::size_t y) -> const float* {
+    const unsigned char* src = static_cast<const unsigned char*>(pixels) + y * stride;
+    const cudaError_t e = cudaMemcpyAsync(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) {
+      const cudaError_t e2 = cudaStreamSynchronize(s);
+      if (e2 != cudaSuccess) fetch_error = e2;
+    } else {
+      fetch_error = e;
+    }
+    if (layout == RDB_RGBAF32) {
+      std::memcpy(widened.data(), raw.data(), raw.size());
+    } else {
+      for (std::size_t x = 0; x < W; ++x) {
+        widened[4 * x + 0] = static_cast<float>(raw[bpp * x + 0]) * 257.0f;
+        widened[4 * x + 1] = static_cast<float>(raw[bpp * x + 1]) * 257.0f;
+        widened[4 * x + 2] = static_cast<float>(raw[bpp * x + 2]) * 257.0f;
+        widened[4 * x + 3] = bpp == 4 ? static_cast<float>(raw[bpp * x + 3]) * 257.0f : 65535.0f;
+      }
+    }
+    return widened.data();
+  };
+  const std::size_t H = static_cast<std::size_t>(height);
+  const std::size_t y0 = out->Begin(row_at, W, H, max_colors, assoc, gray);
+  if (fetch_error != cudaSuccess) return CudaFail(fetch_error, "octree row fetch");
+  if (y0 < H) {
+    // The first loop's live nodes, by key, to start the second from.
+    std::vector<uint64_t> keys;
+    std::vector<int32_t> index;
+    out->LiveKeys(&keys, &index);
+    std::vector<std::size_t> order(keys.size());
+    for (std::size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) { return keys[a] < keys[b]; });
+    const std::size_t n = keys.size();
+    std::vector<uint64_t> k_sorted(n), count(n);
+    std::vector<double> qerr(n), total(4 * n);
+    for (std::size_t i = 0; i < n; ++i) {
+      const OctNode& node = out->nodes()[static_cast<std::size_t>(index[order[i]])];
+      k_sorted[i] = keys[order[i]];
+      qerr[i] = node.qerr;
+      count[i] = node.number_unique;
+      for (int c = 0; c < 4; ++c) total[4 * i + c] = node.total[c];
+    }
+    const std::size_t init_bytes = n * (8 + 8 + 8 + 32) + 256;
+    if (int rc = Reserve(&octree_init_, init_bytes, "octree seed")) return rc;
+    unsigned char* ib = static_cast<unsigned char*>(octree_init_.ptr);
+    OctreeRowsLaunch L{};
+    L.pixels = static_cast<const unsigned char*>(pixels);
+    L.row_stride = static_cast<int64_t>(stride);
+    L.width = width;
+    L.y0 = static_cast<int64_t>(y0);
+    L.pixels_n = static_cast<int64_t>(W * (H - y0));
+    L.layout = layout;
+    L.assoc = assoc ? 1 : 0;
+    L.levels = out->depth();
+    L.init_n = static_cast<int>(n);
+    L.init_keys = reinterpret_cast<const uint64_t*>(ib);
+    L.init_qerr = reinterpret_cast<const double*>(ib + n * 8);
+    L.init_count = reinterpret_cast<const uint64_t*>(ib + n * 16);
+    L.init_total = reinterpret_cast<const double*>(ib + n * 24);
+    cudaError_t e = cudaSuccess;
+    if (n && ((e = cudaMemcpyAsync(ib, k_sorted.data(), n * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+              (e = cudaMemcpyAsync(ib + n * 8, qerr.data(), n * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+              (e = cudaMemcpyAsync(ib + n * 16, count.data(), n * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+              (e = cudaMemcpyAsync(ib + n * 24, total.data(), n * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess)) {
+      return CudaFail(e, "octree seed upload");
+    }
+    const std::size_t scratch = OctreeRowsScratch(L.pixels_n, L.levels);
+    if (int rc = Reserve(&octree_scratch_, scratch, "octree classification")) return rc;
+    OctreeRows rows;
+    if ((e = ClassifyRowsDevice(L, octree_scratch_.ptr, scratch, s, &rows)) != cudaSuccess) {
+      return CudaFail(e, "octree classification");
+    }
+    if (out->Absorb(rows)) {
+      *device_rows = static_cast<int>(H - y0);
+    } else {
+      out->ClassifyRows(row_at, W, y0, H);
+      if (fetch_error != cudaSuccess) return CudaFail(fetch_error, "octree row fetch");
+    }
+  }
+  out->Finish();
   return RDB_OK;
 }
 

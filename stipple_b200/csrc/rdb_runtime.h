@@ -13,6 +13,7 @@
 
 #include "../../include/rdb.h"
 #include "rdb_plan.h"
+#include "rdb_octree.h"
 #include "rdb_walk.h"
 
 namespace rdb {
@@ -84,6 +85,13 @@ class Context {
   // alpha only.
   int Candidates(int id, cudaStream_t s, const uint32_t** out);
   int DumpBlockIndices(const BlockLaunch& L, int64_t positions, cudaStream_t s);
+  // ColorTree::Build of an image in device memory (rdb_octree_build_device):
+  // the first classification loop on the host over rows copied back, the
+  // second on the device (rdb_octree_dev.cu), the reduction on the host.
+  // *device_rows receives how many rows the device classified.
+  int BuildOctree(const void* pixels, int layout, int width, int height, std::size_t row_stride,
+                  int max_colors, bool assoc, bool gray, cudaStream_t s, Octree* out,
+                  int* device_rows);
 
   // Visit order of a geometry, built on first use and kept resident.
   int Order(int width, int height, cudaStream_t s, const int32_t** out);
@@ -177,6 +185,8 @@ class Context {
   bool profiling_ = false;
   std::string dump_prefix_;   // rdb_context_dump_indices: "" = off
   DevBuf dump_buf_;
+  DevBuf octree_scratch_;
+  DevBuf octree_init_;
   rdb_kernel_stats stats_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};
   // Pipelined pass loop of the segmented walk: a pinned ring of per-pass
