@@ -1416,6 +1416,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   if (int rc = Reserve(&tsw_q_, 3 * q_bytes, "segment queues")) return rc;
   if (int rc = Reserve(&tsw_cx_, static_cast<std::size_t>(positions) * (is_float ? 16 : 4), "gathered samples")) return rc;
   if (int rc = Reserve(&tsw_chosen_, static_cast<std::size_t>(positions), "segment indices")) return rc;
+  if (int rc = Reserve(&tsw_changed_, static_cast<std::size_t>(total), "segment queue flags")) return rc;
   if (use_cache) {
     if (int rc = Reserve(&tsw_own_, own_entries * sizeof(uint64_t), "segment memo tables")) return rc;
     if (int rc = Reserve(&tsw_list_, own_entries * sizeof(uint32_t), "segment memo lists")) return rc;
@@ -1469,6 +1470,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.chunk_threads = kChunk;
   L.bad[0] = bad;
   L.bad[1] = bad + n;
+  L.changed = static_cast<uint8_t*>(tsw_changed_.ptr);
   L.status = static_cast<int*>(status_.ptr);
   scaled_weights(o.diffusion, L.sw);
 

@@ -186,6 +186,7 @@ class Context {
   std::string dump_prefix_;   // rdb_context_dump_indices: "" = off
   DevBuf dump_buf_;
   DevBuf octree_scratch_;
+  DevBuf tsw_changed_;
   DevBuf octree_init_;
   rdb_kernel_stats stats_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};

@@ -247,6 +247,8 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   uint32_t* hkeys = im.hkeys;
   const uint32_t hmask = im.hmask;
   const int warp_steps = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(steps));
+  const double* qold = L.q_end[(L.pass & 1) ^ 1] + static_cast<int64_t>(sid) * 64;
+  bool changed = false;
   int n_own = 0;
   uint32_t acc = 0;
 #pragma unroll 1
@@ -414,8 +416,13 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
         }
         if (t >= end - 16) {
           double* d = qe + 4 * (t - (end - 16));
+          const double* o = qold + 4 * (t - (end - 16));
 #pragma unroll
-          for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
+          for (int c = 0; c < 4; ++c) {
+            const double v = c < C ? e[c < C ? c : 0] : 0.0;
+            changed |= __double_as_longlong(o[c]) != __double_as_longlong(v);
+            d[c] = v;
+          }
         }
       } else if (t >= begin - 16) {
         double* d = qs + 4 * (t - (begin - 16));
@@ -425,6 +432,7 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     }
   }
   if (active && memo) L.own_count[sid] = n_own;
+  if (active) L.changed[sid] = changed ? 1 : 0;
 }
 
 template <bool kFloat, bool kAssoc>
@@ -466,13 +474,15 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   WalkSegment<kFloat, kAssoc>(L, im, P, errp, active ? k : warp_end - 1, active, lane);
 }
 
-// G_new = the entries of G_prev that verified segments made; usemin cleared.
+// G_new = the entries of G_prev that verified segments made; usemin cleared;
+// this pass's first failure of the image reset to "none".
 // Direct maps: one thread per key; hashed maps: the inserted slots.
 __global__ void TswPrepare(TswLaunch L) {
   const int m = blockIdx.y;
   if (m >= L.n_images) return;
   const TswImage& im = L.images[m];
   const int front = front_of(L, m, im.nsegs);
+  if (blockIdx.x == 0 && threadIdx.x == 0) L.bad[L.pass & 1][m] = 0x7F7F7F7F;
   const uint32_t* gp = im.g[(L.pass & 1) ^ 1];
   uint32_t* gn = im.g[L.pass & 1];
   const int stride = gridDim.x * blockDim.x;
@@ -543,12 +553,18 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
   if (k > *reinterpret_cast<volatile const int*>(L.bad[L.pass & 1] + lo)) return;
   bool ok = true;
   if (k > front) {
-    // The first walked segment started from a verified predecessor's queue.
-    const double* a = (L.pass == 0) ? L.q_start + static_cast<int64_t>(sid) * 64
-                                    : L.q_end[(L.pass & 1) ^ 1] + static_cast<int64_t>(sid - 1) * 64;
-    const double* b = L.q_end[L.pass & 1] + static_cast<int64_t>(sid - 1) * 64;
-    for (int i = lane; i < 64; i += 32) {
-      if (__double_as_longlong(a[i]) != __double_as_longlong(b[i])) ok = false;
+    // The first walked segment started from a verified predecessor's queue;
+    // the others from their predecessor's end queue of the previous pass,
+    // which the predecessor compared with its new one (L.changed).  Pass 0
+    // started from warm-ups and compares the queues themselves.
+    if (L.pass == 0) {
+      const double* a = L.q_start + static_cast<int64_t>(sid) * 64;
+      const double* b = L.q_end[0] + static_cast<int64_t>(sid - 1) * 64;
+      for (int i = lane; i < 64; i += 32) {
+        if (__double_as_longlong(a[i]) != __double_as_longlong(b[i])) ok = false;
+      }
+    } else if (L.changed[sid - 1]) {
+      ok = false;
     }
   }
   if (L.use_cache) {
@@ -719,16 +735,20 @@ const void* WalkFunc() {
 // walk, check, control.
 cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int total_segs,
                     cudaGraphConditionalHandle* h, int** ctl, uint32_t** tag_dev, int* max_passes) {
-  cudaMemsetParams ms{};
-  ms.dst = L->bad[L->pass & 1];
-  ms.value = 0x7F;
-  ms.elementSize = 1;
-  ms.width = static_cast<std::size_t>(L->n_images) * sizeof(int);
-  ms.height = 1;
-  cudaGraphNode_t node;
-  cudaError_t e = cudaGraphAddMemsetNode(&node, g, *last ? last : nullptr, *last ? 1 : 0, &ms);
-  if (e != cudaSuccess) return e;
-  *last = node;
+  cudaError_t e;
+  if (!L->use_cache || L->n_images <= 0) {
+    // Without the memo no prepare kernel runs to reset this pass's failures.
+    cudaMemsetParams ms{};
+    ms.dst = L->bad[L->pass & 1];
+    ms.value = 0x7F;
+    ms.elementSize = 1;
+    ms.width = static_cast<std::size_t>(L->n_images) * sizeof(int);
+    ms.height = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddMemsetNode(&node, g, *last ? last : nullptr, *last ? 1 : 0, &ms);
+    if (e != cudaSuccess) return e;
+    *last = node;
+  }
   void* args1[] = {L};
   if (L->use_cache && L->n_images > 0) {
     e = AddKernel(g, last, reinterpret_cast<const void*>(TswPrepare), dim3(kKeys / 256, L->n_images),

@@ -99,6 +99,11 @@ struct TswLaunch {
   // = none).  Pass p walks from min(bad[(p-1) & 1], nsegs) -- its verified
   // prefix -- and writes bad[p & 1].
   int* bad[2];
+  // Per segment, written by every walk from pass 1 on: 1 when the segment's end
+  // queue differs from the one it ended with in the previous pass -- exactly
+  // when the next segment, which started from that previous queue, started
+  // from the wrong one.
+  uint8_t* changed;
   int* status;
   // Device-side loop: the own-table tag of the running pass (null: use `tag`).
   const uint32_t* tag_dev;
