@@ -137,6 +137,10 @@ size_t rdb_context_bytes(const rdb_context* ctx);
  * any; 1 when every segment's speculation held on the first pass).  No
  * reference counterpart: the reference walks one chain. */
 int rdb_context_last_passes(const rdb_context* ctx);
+/* Sweeps the last block-sweep approximation (rdb_options.jacobi_form 0) ran on
+ * this context, and whether its last sweep changed no block's end queue (so
+ * its result is exactly the cache-free walk).  No reference counterpart. */
+int rdb_context_last_sweeps(const rdb_context* ctx, int* converged);
 
 /* Device-side counters of the segmented sequential walk, kept while profiling
  * is on (rdb_context_profile(ctx, 1) clears them).  Walk-kernel times are CUDA
@@ -253,7 +257,17 @@ typedef struct rdb_options {
                            node repeats the passes until a control kernel sees convergence,
                            so the call returns without waiting for the device (errors then
                            surface at rdb_synchronize) */
-  int reserved[3];
+  int jacobi_form;      /* approximation engine (RDB_ENGINE_JACOBI): 0 = block sweeps (default):
+                           the block-mode list cut into blocks of 256 positions, every block
+                           walked in parallel, cache-free, each starting from its
+                           predecessor's end queue of the previous sweep (zeros in the first),
+                           up to jacobi_iters sweeps and stopping at the first sweep in which
+                           no block's end queue changed -- from then on the result is exactly
+                           the cache-free walk along the block-mode list (the reference's walk
+                           with its memo table off); 1 = the point iteration with the
+                           truncated inverse filter (jacobi_taps, jacobi_fp64), as the
+                           reference's approx engine */
+  int reserved[2];
 } rdb_options;
 
 void rdb_options_default(rdb_options* o);

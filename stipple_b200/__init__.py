@@ -52,7 +52,8 @@ class Options(C.Structure):
         ("warm_len", C.c_int),
         ("max_passes", C.c_int),
         ("loop_mode", C.c_int),
-        ("reserved", C.c_int * 3),
+        ("jacobi_form", C.c_int),
+        ("reserved", C.c_int * 2),
     ]
 
 
@@ -170,6 +171,7 @@ SIGNATURES = {
     "rdb_context_destroy": (None, [C.c_void_p]),
     "rdb_context_bytes": (C.c_size_t, [C.c_void_p]),
     "rdb_context_last_passes": (C.c_int, [C.c_void_p]),
+    "rdb_context_last_sweeps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "rdb_server_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "rdb_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
     "rdb_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p]),
@@ -336,6 +338,13 @@ class Context:
     def last_passes(self) -> int:
         """Passes the last segmented sequential walk took."""
         return load().rdb_context_last_passes(self.handle)
+
+    @property
+    def last_sweeps(self) -> tuple[int, bool]:
+        """(sweeps, converged) of the last block-sweep approximation."""
+        conv = C.c_int(0)
+        n = load().rdb_context_last_sweeps(self.handle, C.byref(conv))
+        return n, bool(conv.value)
 
     def dump_indices(self, prefix: str | None) -> None:
         """rdb_context_dump_indices: block walks write `<prefix>.idx.bin`."""

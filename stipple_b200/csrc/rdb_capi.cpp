@@ -256,6 +256,12 @@ void rdb_context_destroy(rdb_context* ctx) { delete ctx; }
 
 size_t rdb_context_bytes(const rdb_context* ctx) { return ctx ? ctx->impl.bytes() : 0; }
 
+int rdb_context_last_sweeps(const rdb_context* ctx, int* converged) {
+  if (!ctx) return 0;
+  if (converged) *converged = ctx->impl.last_sweeps_converged() ? 1 : 0;
+  return ctx->impl.last_sweeps();
+}
+
 int rdb_context_last_passes(const rdb_context* ctx) {
   return ctx ? const_cast<rdb_context*>(ctx)->impl.last_passes() : 0;
 }

@@ -580,7 +580,7 @@ int Context::Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream
 // Shared by rdb_dither's blocks engine and the video-frame form: `imgs` hold
 // everything but the walk bookkeeping, which is filled in here.
 int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const rdb_options& o,
-                       cudaStream_t s) {
+                       cudaStream_t s, int sweeps) {
   if (o.block < kQueue) {
     return Fail(RDB_E_UNSUPPORTED, "--blocks must be at least 16 (the error queue is 16 entries deep)");
   }
@@ -643,9 +643,84 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
   L.is_float = packed ? 0 : 1;
   scaled_weights(o.diffusion, L.sw);
   L.status = static_cast<int*>(status_.ptr);
-  e = LaunchBlockWalk(L, positions, s);
-  if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
+  if (sweeps <= 1) {
+    e = LaunchBlockWalk(L, positions, s);
+    if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
+    if (!dump_prefix_.empty()) return DumpBlockIndices(L, positions, s);
+    return RDB_OK;
+  }
+  // Block sweeps: end queues ping-pong between two buffers; the counter of
+  // changed blocks sits after them.
+  const std::size_t qbytes = static_cast<std::size_t>(blocks) * 64 * sizeof(double);
+  if (int rc = Reserve(&sweep_q_, 2 * qbytes + 256, "block sweep queues")) return rc;
+  double* qbuf[2] = {static_cast<double*>(sweep_q_.ptr),
+                     reinterpret_cast<double*>(static_cast<unsigned char*>(sweep_q_.ptr) + qbytes)};
+  int* changed = reinterpret_cast<int*>(static_cast<unsigned char*>(sweep_q_.ptr) + 2 * qbytes);
+  if ((e = LaunchBlockGather(L, s)) != cudaSuccess) return CudaFail(e, "block sweep gather");
+  last_sweeps_ = 0;
+  last_sweeps_converged_ = false;
+  for (int k = 0; k < sweeps; ++k) {
+    L.q_in = k == 0 ? nullptr : qbuf[(k - 1) & 1];
+    L.q_out = qbuf[k & 1];
+    L.changed = changed;
+    if ((e = cudaMemsetAsync(changed, 0, sizeof(int), s)) != cudaSuccess ||
+        (e = LaunchBlockWalkOnly(L, s)) != cudaSuccess) {
+      return CudaFail(e, "block sweep");
+    }
+    last_sweeps_ = k + 1;
+    if (k == 0) continue;
+    int n_changed = 0;
+    if ((e = cudaMemcpyAsync(&n_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+      return CudaFail(e, "block sweep check");
+    }
+    if (n_changed == 0) {
+      last_sweeps_converged_ = true;
+      break;
+    }
+  }
+  if (sweeps == 1 || blocks == static_cast<int64_t>(imgs.size())) last_sweeps_converged_ = true;
+  if ((e = LaunchBlockScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "block sweep scatter");
   if (!dump_prefix_.empty()) return DumpBlockIndices(L, positions, s);
+  return RDB_OK;
+}
+
+// The approximation's default form (rdb_options.jacobi_form 0): block sweeps
+// over each image's block-mode list, blocks of 256, images of one palette and
+// layout walked together.
+int Context::JacobiSweeps(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
+  if (o.jacobi_iters < 0) return Fail(RDB_E_INVALID, "negative Jacobi iteration count");
+  rdb_options bo = o;
+  bo.block = 256;
+  const int sweeps = std::max(1, o.jacobi_iters);
+  int most = 0;
+  bool all_converged = true;
+  int i = 0;
+  while (i < n) {
+    int k = i + 1;
+    while (k < n && jobs[k].palette_id == jobs[i].palette_id && jobs[k].layout == jobs[i].layout) ++k;
+    std::vector<BlockImage> imgs(static_cast<std::size_t>(k - i));
+    for (int m = i; m < k; ++m) {
+      const rdb_job& j = jobs[m];
+      BlockImage& b = imgs[static_cast<std::size_t>(m - i)];
+      b.pixels = static_cast<const unsigned char*>(j.pixels);
+      b.row_stride = static_cast<int64_t>(RowStride(j));
+      b.width = j.width;
+      b.height = j.height;
+      b.layout = j.layout;
+      b.indices = j.indices;
+      b.rgba_out = reinterpret_cast<float4*>(j.rgba_out);
+      if (j.rgba_out == j.pixels && BlockListLength(j.width, j.height) == 0) b.rgba_out = nullptr;
+    }
+    last_sweeps_ = 0;
+    last_sweeps_converged_ = true;  // an image with an empty list needs no sweep
+    if (int rc = RunBlocks(jobs[i].palette_id, jobs[i].layout, imgs, bo, s, sweeps)) return rc;
+    most = std::max(most, last_sweeps_);
+    all_converged = all_converged && last_sweeps_converged_;
+    i = k;
+  }
+  last_sweeps_ = most;
+  last_sweeps_converged_ = all_converged;
   return RDB_OK;
 }
 
@@ -917,6 +992,8 @@ int Context::FramesHost(const rdb_frames& f, const rdb_options& o) {
 
 int Context::Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s) {
   if (o.jacobi_taps < 1 || o.jacobi_taps > 4096) return Fail(RDB_E_UNSUPPORTED, "--approx-taps out of range");
+  if (o.jacobi_form != 0 && o.jacobi_form != 1) return Fail(RDB_E_INVALID, "jacobi_form must be 0 or 1");
+  if (o.jacobi_form == 0) return JacobiSweeps(jobs, n, o, s);
   if (o.jacobi_iters < 0) return Fail(RDB_E_INVALID, "negative Jacobi iteration count");
   // Impulse response of F = (I - H)^-1 for the walk's own feedback.  The walk
   // adds sw[i] * error[i] with error[15] the newest residual

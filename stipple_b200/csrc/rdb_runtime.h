@@ -117,8 +117,11 @@ class Context {
   int SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int SeqAuto(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int Blocks(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
+  // `sweeps` > 1: block sweeps (rdb_options.jacobi_form 0), stopping early at
+  // the first sweep that changes no block's end queue.
   int RunBlocks(int pid, int layout, std::vector<BlockImage>& imgs, const rdb_options& o,
-                cudaStream_t s);
+                cudaStream_t s, int sweeps = 1);
+  int JacobiSweeps(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int CheckFrames(const rdb_frames& f) const;
   int Jacobi(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int CheckJob(const rdb_job& j) const;
@@ -187,6 +190,9 @@ class Context {
   DevBuf dump_buf_;
   DevBuf octree_scratch_;
   DevBuf tsw_changed_;
+  DevBuf sweep_q_;
+  int last_sweeps_ = 0;
+  bool last_sweeps_converged_ = false;
   DevBuf octree_init_;
   rdb_kernel_stats stats_{};
   cudaEvent_t ev_[2] = {nullptr, nullptr};
@@ -213,6 +219,8 @@ class Context {
   // Passes of the last segmented walk; after a device-side loop this waits
   // for that call's stream and reads the loop's own count.
   int last_passes();
+  int last_sweeps() const { return last_sweeps_; }
+  bool last_sweeps_converged() const { return last_sweeps_converged_; }
   int Profile(bool on);
   // Block walks write `<prefix>.idx.bin` (every image's chosen index at every
   // block-list position, in list order, images in call order); "" = off.

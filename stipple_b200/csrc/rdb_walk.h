@@ -92,11 +92,26 @@ struct BlockLaunch {
   int is_float;                 // cx holds the sample widened to float4 (every layout but
                                 // RGB8 / RGBA8, which pack into one word)
   int bpad;                     // positions per block in the scratch (multiple of 16)
+  // Block sweeps (the Jacobi engine's default form): each block starts from
+  // its predecessor's end queue of the previous sweep, q_in[(block - 1) * 64 ..]
+  // (16 entries of 4 doubles, oldest first), where the predecessor is in the
+  // same image; blocks that start an image, and every block when q_in is
+  // null, start from zeros.  Each block writes its end queue to q_out
+  // (when not null) and, when q_in is not null, counts into *changed the
+  // blocks with a successor whose end queue differs from their q_in entry.
+  const double* q_in;
+  double* q_out;
+  int* changed;
   double sw[16];
   int* status;
 };
 
 cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream);
+// The three phases of LaunchBlockWalk separately (block sweeps walk many times
+// between one gather and one scatter).
+cudaError_t LaunchBlockGather(const BlockLaunch& L, cudaStream_t stream);
+cudaError_t LaunchBlockWalkOnly(const BlockLaunch& L, cudaStream_t stream);
+cudaError_t LaunchBlockScatter(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream);
 // The chosen index of every position of every image, in list order, images
 // back to back (`out`: total_positions bytes).
 cudaError_t LaunchBlockChosenLinear(const BlockLaunch& L, int64_t total_positions, uint8_t* out,

@@ -276,8 +276,11 @@ __device__ __forceinline__ uint32_t pick(const uint4& q, int k) {
 // key's survivors from the candidate table when the palette has one (the
 // full descent and search only for keys the table does not cover).
 template <bool kAssoc, bool kFloat>
-__device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& P, int64_t g,
-                                          int lane, int len) {
+__device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& P, int64_t gb,
+                                          const BlockRef& ref) {
+  const int64_t g = gb >> 5;
+  const int lane = static_cast<int>(gb & 31);
+  const int len = ref.len;
   constexpr int C = kAssoc ? 4 : 3;
   const uint4* cx4 = reinterpret_cast<const uint4*>(L.cx) + g * (L.bpad >> 2) * 32 + lane;
   const float4* cxf = reinterpret_cast<const float4*>(L.cx) + g * L.bpad * 32 + lane;
@@ -299,6 +302,27 @@ __device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& 
       for (int c = 0; c < C; ++c) R[4 * q + k][c] = p[c];
     }
   }
+  const int b = ref.begin / L.block;            // block index within its image
+  const bool has_next = b + 1 < ref.im->nblocks;
+  if (L.q_in && b > 0) {
+    // Start from the predecessor's end queue q[0..15] (oldest first): pixel j
+    // holds p + sum_{m=j}^{14} w_{m-j} q[m] in ascending m, and q[15] is the
+    // pending residual.
+    const double* q = L.q_in + (gb - 1) * 64;
+#pragma unroll
+    for (int m = 0; m < 15; ++m) {
+#pragma unroll
+      for (int j = 0; j <= m; ++j) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) R[j][c] = __dadd_rn(R[j][c], __dmul_rn(L.sw[m - j], q[4 * m + c]));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) e[c] = q[60 + c];
+  }
+  double* qo = L.q_out ? L.q_out + gb * 64 : nullptr;
+  const double* qp = (L.q_in && has_next) ? L.q_in + gb * 64 : nullptr;
+  bool changed = false;
   uint4 ahead = make_uint4(0u, 0u, 0u, 0u);  // packed samples t+16 .. t+19
   uint32_t acc[4] = {0u, 0u, 0u, 0u};
   int u = 0;
@@ -364,6 +388,15 @@ __device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& 
     const double* rc = P.rcol<kAssoc>(index);
 #pragma unroll
     for (int k = 0; k < C; ++k) e[k] = __dadd_rn(static_cast<double>(f[k]), -rc[k]);
+    if (qo && t >= len - 16) {
+      const int at = 4 * (t - (len - 16));
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const double v = c < C ? e[c < C ? c : 0] : 0.0;
+        if (qp) changed |= __double_as_longlong(qp[at + c]) != __double_as_longlong(v);
+        qo[at + c] = v;
+      }
+    }
     const int q = (t >> 2) & 3;
     const uint32_t bits = static_cast<uint32_t>(index) << (8 * (t & 3));
     if (q == 0) acc[0] |= bits; else if (q == 1) acc[1] |= bits; else if (q == 2) acc[2] |= bits; else acc[3] |= bits;
@@ -372,6 +405,7 @@ __device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& 
       acc[0] = acc[1] = acc[2] = acc[3] = 0u;
     }
   }
+  if (changed && L.changed) atomicAdd(L.changed, 1);
 }
 template <bool kAssoc, bool kFloat>
 __global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaunch L) {
@@ -387,7 +421,7 @@ __global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaun
   tw::Plan P;
   P.bind(smem);
   const BlockRef r = block_ref(L, gb);
-  WalkBlock<kAssoc, kFloat>(L, P, gb >> 5, static_cast<int>(gb & 31), r.len);
+  WalkBlock<kAssoc, kFloat>(L, P, gb, r);
 }
 
 template <bool kAssoc, bool kFloat>
@@ -502,20 +536,35 @@ cudaError_t LaunchBlockChosenLinear(const BlockLaunch& L, int64_t total_position
   return cudaGetLastError();
 }
 
-cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
-  if (total_positions <= 0 || L.total_blocks <= 0) return cudaSuccess;
+cudaError_t LaunchBlockGather(const BlockLaunch& L, cudaStream_t stream) {
+  if (L.total_blocks <= 0) return cudaSuccess;
   const int64_t cells = (L.total_blocks + 31) / 32 * 32 * L.bpad;  // positions in the scratch
   if (L.is_float) {
     BlockGatherWide<<<static_cast<unsigned>((cells + 255) / 256), 256, 0, stream>>>(L, cells);
   } else {
     BlockGatherPacked<<<static_cast<unsigned>((cells / 4 + 255) / 256), 256, 0, stream>>>(L, cells / 4);
   }
-  const unsigned g1 = static_cast<unsigned>((total_positions + 255) / 256);
-  cudaError_t e = L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, stream) : LaunchWalk<true, false>(L, stream))
-                          : (L.is_float ? LaunchWalk<false, true>(L, stream) : LaunchWalk<false, false>(L, stream));
-  if (e != cudaSuccess) return e;
-  BlockScatter<<<g1, 256, 0, stream>>>(L, total_positions);
   return cudaGetLastError();
+}
+
+cudaError_t LaunchBlockWalkOnly(const BlockLaunch& L, cudaStream_t stream) {
+  if (L.total_blocks <= 0) return cudaSuccess;
+  return L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, stream) : LaunchWalk<true, false>(L, stream))
+                 : (L.is_float ? LaunchWalk<false, true>(L, stream) : LaunchWalk<false, false>(L, stream));
+}
+
+cudaError_t LaunchBlockScatter(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
+  if (total_positions <= 0) return cudaSuccess;
+  BlockScatter<<<static_cast<unsigned>((total_positions + 255) / 256), 256, 0, stream>>>(L, total_positions);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
+  if (total_positions <= 0 || L.total_blocks <= 0) return cudaSuccess;
+  cudaError_t e;
+  if ((e = LaunchBlockGather(L, stream)) != cudaSuccess) return e;
+  if ((e = LaunchBlockWalkOnly(L, stream)) != cudaSuccess) return e;
+  return LaunchBlockScatter(L, total_positions, stream);
 }
 
 }  // namespace rdb

@@ -301,6 +301,8 @@ std::string RiemersmaApproxCuda(const Palette& palette, const DitherParams& para
   rdb_options o;
   rdb_options_default(&o);
   o.diffusion = params.diffusion;
+  // The block-sweep form (rdb_options.jacobi_form 0): `iterations` caps the
+  // sweeps; taps and fp64 shape only the point-iteration form.
   o.jacobi_iters = options.iterations;
   o.jacobi_taps = options.taps;
   o.jacobi_fp64 = options.fp64 ? 1 : 0;
