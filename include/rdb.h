@@ -372,8 +372,11 @@ typedef struct rdb_server_options {
   size_t memory_budget;   /* admission cap in bytes (0 = 90 % of free memory) */
   int workers;            /* device workers (0 = 4) */
   int max_batch;          /* requests per batch (0 = 512) */
-  int host_threads;       /* palette builders (0 = the CPUs this process may run on:
-                             its affinity mask, capped by a cgroup CPU quota) */
+  int host_threads;       /* palette builders of the host form (0 = the CPUs this process may
+                             run on: its affinity mask, capped by a cgroup CPU quota) */
+  int host_palettes;      /* 0 (default): each device worker builds its batch's palettes on
+                             the device from the uploaded pixels (rdb_octree_build_device);
+                             1: host threads build them (rdb_octree_build) before admission */
 } rdb_server_options;
 
 typedef struct rdb_request {

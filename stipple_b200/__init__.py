@@ -60,7 +60,7 @@ class Options(C.Structure):
 class ServerOptions(C.Structure):
     """rdb_server_options (include/rdb.h)."""
     _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t), ("workers", C.c_int),
-                ("max_batch", C.c_int), ("host_threads", C.c_int)]
+                ("max_batch", C.c_int), ("host_threads", C.c_int), ("host_palettes", C.c_int)]
 
 
 class Request(C.Structure):
@@ -668,8 +668,8 @@ class Server:
     threads, admits by device memory and batches on its device workers."""
 
     def __init__(self, device: int = 0, budget: int = 0, workers: int = 0, max_batch: int = 0,
-                 host_threads: int = 0):
-        o = ServerOptions(device, budget, workers, max_batch, host_threads)
+                 host_threads: int = 0, host_palettes: bool = False):
+        o = ServerOptions(device, budget, workers, max_batch, host_threads, int(host_palettes))
         self.handle = C.c_void_p()
         _check(load().rdb_server_create(C.byref(o), C.byref(self.handle)))
         self._live: dict[int, tuple] = {}

@@ -327,30 +327,7 @@ int rdb_plan_build(const rdb_palette_desc* d, void* out, size_t cap, size_t* siz
 
 int rdb_palette_from_octree(rdb_context* ctx, const rdb_octree* t, int* palette_id) {
   if (!ctx || !t || !palette_id) return Guard("rdb_palette_from_octree");
-  const auto& nodes = t->tree.nodes();
-  const auto& cm = t->tree.colormap();
-  std::vector<double> colors(cm.size() * 4);
-  for (std::size_t i = 0; i < cm.size(); ++i) {
-    colors[4 * i] = cm[i].r;
-    colors[4 * i + 1] = cm[i].g;
-    colors[4 * i + 2] = cm[i].b;
-    colors[4 * i + 3] = cm[i].a;
-  }
-  std::vector<int32_t> child(nodes.size() * 16), parent(nodes.size());
-  std::vector<uint32_t> cn(nodes.size());
-  std::vector<uint64_t> nu(nodes.size());
-  rdb_octree_nodes(t, child.data(), parent.data(), cn.data(), nu.data());
-  rdb::PlanInput in;
-  in.count = t->tree.color_count();
-  in.assoc = t->tree.associate_alpha();
-  in.colors = colors.data();
-  in.node_count = static_cast<int>(nodes.size());
-  in.root = 0;
-  in.child = child.data();
-  in.parent = parent.data();
-  in.color_number = cn.data();
-  in.number_unique = nu.data();
-  return ctx->impl.CreatePalette(in, palette_id);
+  return ctx->impl.CreatePaletteFromTree(t->tree, palette_id);
 }
 
 int rdb_palette_destroy(rdb_context* ctx, int palette_id) {

@@ -208,16 +208,36 @@ std::size_t OctreeRowsTemp(int64_t P, int levels) {
   return most;
 }
 
+// Bounds on the distinct keys of a launch: nodes of levels 1..levels (and
+// leaves at the last level) of a tree of the given fan-out, at most one per
+// element.
+int64_t NodeBound(int64_t elements, int levels, int fan) {
+  int64_t total = 0, at = 1;
+  for (int l = 1; l <= levels && total < elements; ++l) {
+    at = at > elements ? at : at * fan;
+    total += at;
+  }
+  return total < elements ? total : elements;
+}
+int64_t LeafBound(int64_t runs, int levels, int fan) {
+  int64_t at = 1;
+  for (int l = 1; l <= levels && at < runs; ++l) at *= fan;
+  return at < runs ? at : runs;
+}
+
 }  // namespace
 
-std::size_t OctreeRowsScratch(int64_t pixels, int levels) {
+std::size_t OctreeRowsScratch(int64_t pixels, int levels, bool assoc) {
+  const int fan = assoc ? 16 : 8;
   const std::size_t P = static_cast<std::size_t>(pixels);
   const std::size_t E = P * static_cast<std::size_t>(levels);
+  const std::size_t U = static_cast<std::size_t>(NodeBound(static_cast<int64_t>(E), levels, fan));
+  const std::size_t UL = static_cast<std::size_t>(LeafBound(pixels, levels, fan));
   // flag, id, first (int, P); keys x2, vals x2 (E); leaf keys x2, leaf runs x2
-  // (P); unique keys, counts, offsets, errors, gains (E); leaf keys, counts,
-  // offsets, numbers, totals (P); CUB temp; alignment slack.
-  return 3 * P * 4 + 4 * E * 8 + 2 * P * 8 + 2 * P * 4 + E * (8 + 4 + 4 + 8 + 8) +
-         P * (8 + 4 + 4 + 8 + 32) + OctreeRowsTemp(pixels, levels) + 64 * 256;
+  // (P); unique keys, counts, offsets, errors, gains (U); leaf keys, counts,
+  // offsets, numbers, totals (UL); CUB temp; alignment slack.
+  return 3 * P * 4 + 4 * E * 8 + 2 * P * 8 + 2 * P * 4 + U * (8 + 4 + 4 + 8 + 8) +
+         UL * (8 + 4 + 4 + 8 + 32) + OctreeRowsTemp(pixels, levels) + 64 * 256;
 }
 
 cudaError_t ClassifyRowsDevice(const OctreeRowsLaunch& L, void* scratch, std::size_t scratch_bytes,
@@ -244,16 +264,19 @@ cudaError_t ClassifyRowsDevice(const OctreeRowsLaunch& L, void* scratch, std::si
   uint64_t* lkeys2 = static_cast<uint64_t*>(take(P * 8));
   int* lruns = static_cast<int*>(take(P * 4));
   int* lruns2 = static_cast<int*>(take(P * 4));
-  uint64_t* ukeys = static_cast<uint64_t*>(take(E0 * 8));
-  int* ucount = static_cast<int*>(take(E0 * 4));
-  int* uoff = static_cast<int*>(take(E0 * 4));
-  double* qerr = static_cast<double*>(take(E0 * 8));
-  double* gain = static_cast<double*>(take(E0 * 8));
-  uint64_t* lukeys = static_cast<uint64_t*>(take(P * 8));
-  int* lcount = static_cast<int*>(take(P * 4));
-  int* loff = static_cast<int*>(take(P * 4));
-  uint64_t* lnum = static_cast<uint64_t*>(take(P * 8));
-  double* ltot = static_cast<double*>(take(P * 32));
+  const int fan = L.assoc ? 16 : 8;
+  const int64_t U = NodeBound(E0, L.levels, fan);
+  const int64_t UL = LeafBound(P, L.levels, fan);
+  uint64_t* ukeys = static_cast<uint64_t*>(take(U * 8));
+  int* ucount = static_cast<int*>(take(U * 4));
+  int* uoff = static_cast<int*>(take(U * 4));
+  double* qerr = static_cast<double*>(take(U * 8));
+  double* gain = static_cast<double*>(take(U * 8));
+  uint64_t* lukeys = static_cast<uint64_t*>(take(UL * 8));
+  int* lcount = static_cast<int*>(take(UL * 4));
+  int* loff = static_cast<int*>(take(UL * 4));
+  uint64_t* lnum = static_cast<uint64_t*>(take(UL * 8));
+  double* ltot = static_cast<double*>(take(UL * 32));
   int* nseg = static_cast<int*>(take(2 * sizeof(int)));
   void* temp = take(0);
   if (used > scratch_bytes) return cudaErrorMemoryAllocation;

@@ -28,7 +28,7 @@ struct OctreeRowsLaunch {
 };
 
 // Device bytes the loop needs for `pixels` pixels at `levels` levels.
-std::size_t OctreeRowsScratch(int64_t pixels, int levels);
+std::size_t OctreeRowsScratch(int64_t pixels, int levels, bool assoc);
 // Runs the loop and copies its result to the host (synchronous on `s`).
 cudaError_t ClassifyRowsDevice(const OctreeRowsLaunch& L, void* scratch, std::size_t scratch_bytes,
                                cudaStream_t s, OctreeRows* out);

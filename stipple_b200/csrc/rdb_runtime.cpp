@@ -2,6 +2,7 @@
 #include "rdb_runtime.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <map>
 #include <tuple>
@@ -802,7 +803,7 @@ int Context::BuildOctree(const void* pixels, int layout, int width, int height, 
               (e = cudaMemcpyAsync(ib + n * 24, total.data(), n * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess)) {
       return CudaFail(e, "octree seed upload");
     }
-    const std::size_t scratch = OctreeRowsScratch(L.pixels_n, L.levels);
+    const std::size_t scratch = OctreeRowsScratch(L.pixels_n, L.levels, assoc);
     if (int rc = Reserve(&octree_scratch_, scratch, "octree classification")) return rc;
     OctreeRows rows;
     if ((e = ClassifyRowsDevice(L, octree_scratch_.ptr, scratch, s, &rows)) != cudaSuccess) {
@@ -1076,9 +1077,10 @@ int Context::Synchronize(cudaStream_t s) {
   return RDB_OK;
 }
 
-int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_options& o) {
+// Host jobs staged back to back on the context's stream (256-byte aligned
+// slices), as device jobs over the staging buffers.
+int Context::StageHostJobs(const rdb_host_job* jobs, int n, std::vector<rdb_job>* out) {
   if (n <= 0) return n == 0 ? RDB_OK : Fail(RDB_E_INVALID, "bad job list");
-  // Stage every job's input back to back (256-byte aligned slices).
   std::vector<std::size_t> in_off(static_cast<std::size_t>(n)), idx_off(static_cast<std::size_t>(n)),
       rgba_off(static_cast<std::size_t>(n));
   std::size_t in_total = 0, idx_total = 0, rgba_total = 0;
@@ -1101,7 +1103,8 @@ int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_o
   if (rgba_total && Reserve(&host_rgba_, rgba_total, "RgbaF staging")) return RDB_E_NOMEM;
   cudaStream_t s = stream_;
   cudaSetDevice(device_);
-  std::vector<rdb_job> dj(static_cast<std::size_t>(n));
+  std::vector<rdb_job>& dj = *out;
+  dj.assign(static_cast<std::size_t>(n), rdb_job{});
   for (int i = 0; i < n; ++i) {
     const rdb_host_job& j = jobs[i];
     const std::size_t row = static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
@@ -1132,7 +1135,12 @@ int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_o
   }
   // Cells an engine leaves unwritten (the block list's gap) read back as 0.
   cudaMemsetAsync(host_idx_.ptr, 0, idx_total, s);
-  if (int rc = Dither(engine, dj.data(), n, o, s)) return rc;
+  return RDB_OK;
+}
+
+// Results of staged host jobs back to their host buffers; waits for them.
+int Context::FinishHostJobs(const rdb_host_job* jobs, int n, const std::vector<rdb_job>& dj) {
+  cudaStream_t s = stream_;
   for (int i = 0; i < n; ++i) {
     const rdb_host_job& j = jobs[i];
     const std::size_t npx = static_cast<std::size_t>(j.width) * j.height;
@@ -1144,6 +1152,82 @@ int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_o
     }
   }
   return Synchronize(s);
+}
+
+int Context::DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_options& o) {
+  std::vector<rdb_job> dj;
+  if (int rc = StageHostJobs(jobs, n, &dj)) return rc;
+  if (n <= 0) return RDB_OK;
+  if (int rc = Dither(engine, dj.data(), n, o, stream_)) return rc;
+  return FinishHostJobs(jobs, n, dj);
+}
+
+int Context::CreatePaletteFromTree(const Octree& t, int* id) {
+  const auto& nodes = t.nodes();
+  const auto& cm = t.colormap();
+  std::vector<double> colors(cm.size() * 4);
+  for (std::size_t i = 0; i < cm.size(); ++i) {
+    colors[4 * i] = cm[i].r;
+    colors[4 * i + 1] = cm[i].g;
+    colors[4 * i + 2] = cm[i].b;
+    colors[4 * i + 3] = cm[i].a;
+  }
+  std::vector<int32_t> child(nodes.size() * 16), parent(nodes.size());
+  std::vector<uint32_t> cn(nodes.size());
+  std::vector<uint64_t> nu(nodes.size());
+  for (std::size_t i = 0; i < nodes.size(); ++i) {
+    for (int c = 0; c < 16; ++c) child[16 * i + c] = nodes[i].child[c];
+    parent[i] = nodes[i].parent;
+    cn[i] = nodes[i].color_number;
+    nu[i] = nodes[i].number_unique;
+  }
+  PlanInput in;
+  in.count = t.color_count();
+  in.assoc = t.associate_alpha();
+  in.colors = colors.data();
+  in.node_count = static_cast<int>(nodes.size());
+  in.root = 0;
+  in.child = child.data();
+  in.parent = parent.data();
+  in.color_number = cn.data();
+  in.number_unique = nu.data();
+  return CreatePalette(in, id);
+}
+
+int Context::DitherHostBuilding(int engine, const rdb_host_job* jobs, const int* colors,
+                                const int* assoc, int n, const rdb_options& o, double* build_ms) {
+  std::vector<rdb_job> dj;
+  if (int rc = StageHostJobs(jobs, n, &dj)) return rc;
+  if (n <= 0) return RDB_OK;
+  std::vector<int> pids;
+  const auto release = [&] {
+    for (int pid : pids) DestroyPalette(pid);
+  };
+  for (int i = 0; i < n; ++i) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const rdb_host_job& j = jobs[i];
+    const int gray = rdb_is_grayscale(j.pixels, j.layout, static_cast<std::size_t>(j.width),
+                                      static_cast<std::size_t>(j.height), j.row_stride);
+    Octree tree;
+    int rows = 0;
+    int rc = BuildOctree(dj[i].pixels, j.layout, j.width, j.height, static_cast<std::size_t>(dj[i].row_stride),
+                         colors[i], assoc[i] != 0, gray != 0, stream_, &tree, &rows);
+    int pid = 0;
+    if (rc == RDB_OK) rc = CreatePaletteFromTree(tree, &pid);
+    if (rc != RDB_OK) {
+      release();
+      return rc;
+    }
+    pids.push_back(pid);
+    dj[static_cast<std::size_t>(i)].palette_id = pid;
+    if (build_ms) {
+      build_ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+  int rc = Dither(engine, dj.data(), n, o, stream_);
+  if (rc == RDB_OK) rc = FinishHostJobs(jobs, n, dj);
+  release();
+  return rc;
 }
 
 // The speculative segmented walk (rdb_ssw.h): every image is cut into

@@ -85,6 +85,8 @@ class Context {
   // alpha only.
   int Candidates(int id, cudaStream_t s, const uint32_t** out);
   int DumpBlockIndices(const BlockLaunch& L, int64_t positions, cudaStream_t s);
+  int StageHostJobs(const rdb_host_job* jobs, int n, std::vector<rdb_job>* out);
+  int FinishHostJobs(const rdb_host_job* jobs, int n, const std::vector<rdb_job>& dj);
   // ColorTree::Build of an image in device memory (rdb_octree_build_device):
   // the first classification loop on the host over rows copied back, the
   // second on the device (rdb_octree_dev.cu), the reduction on the host.
@@ -98,6 +100,12 @@ class Context {
 
   int Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t s);
   int DitherHost(int engine, const rdb_host_job* jobs, int n, const rdb_options& o);
+  // Host jobs whose palettes are built here, each on the device from its own
+  // uploaded pixels (BuildOctree): `colors` and `assoc` per job, their
+  // palette_id ignored; build_ms (may be null) receives each build's time.
+  int DitherHostBuilding(int engine, const rdb_host_job* jobs, const int* colors, const int* assoc,
+                         int n, const rdb_options& o, double* build_ms);
+  int CreatePaletteFromTree(const Octree& t, int* id);
   // Video frames through the blocks engine (rdb_dither_frames).
   int Frames(const rdb_frames& f, const rdb_options& o, cudaStream_t s);
   int FramesHost(const rdb_frames& f, const rdb_options& o);

@@ -1,19 +1,21 @@
 // rdb_serve.cpp -- the request loop declared in include/rdb.h (rdb_server_*).
 //
-// Three stages, each its own threads, joined by queues under one mutex:
-//   build    host threads turn a request into a colour tree (rdb_octree_build,
-//            the reference's ColorTree::Build semantics, greyscale rule of
-//            src/rd_cli.cpp:2452-2456) -- the CPU-heavy part, parallel by
-//            request;
-//   admit    a built request waits until the device-memory estimate of all
+// Stages joined by queues under one mutex:
+//   build    the request's colour tree (the reference's ColorTree::Build
+//            semantics, greyscale rule of src/rd_cli.cpp:2452-2456).  By
+//            default the device worker builds it from the uploaded pixels
+//            (rdb_octree_build_device) at the start of the batch call; with
+//            host_palettes, host threads build it (rdb_octree_build) before
+//            admission, parallel by request;
+//   admit    a request waits until the device-memory estimate of all
 //            admitted requests plus its own fits the budget (first fit in
 //            arrival order, so one large request does not block small ones
 //            behind it forever: it is taken as soon as it fits);
 //   device   each worker owns a context and its stream; when idle it takes
 //            every admitted request that shares the oldest one's engine and
-//            options (and, for the block engine, its palette tree) as one
-//            batched call, so arrivals during a batch form the next batch on
-//            whichever worker frees first.
+//            options (a block request alone: that engine walks one palette
+//            per call) as one batched call, so arrivals during a batch form
+//            the next batch on whichever worker frees first.
 // A request's result does not depend on its batch: every engine treats the
 // jobs of a call independently.
 #include <sched.h>
@@ -32,6 +34,7 @@
 #include <vector>
 
 #include "../../include/rdb.h"
+#include "rdb_octree_dev.h"
 #include "rdb_runtime.h"
 
 namespace {
@@ -88,11 +91,30 @@ struct Req {
   std::string err;
 };
 
+// The octree build's classification depth (rd_octree.cpp:255-275).
+int TreeDepth(int colors, bool assoc, bool gray) {
+  int depth = 1;
+  for (std::size_t c = static_cast<std::size_t>(colors > 0 ? colors : 65536); c != 0; ++depth) c >>= 2;
+  if (depth > 2) --depth;
+  if (assoc && depth > 5) --depth;
+  if (gray) depth = 8;
+  return std::min(8, std::max(2, depth));
+}
+
 // Device bytes one request needs while admitted: staging of input, indices and
 // RgbaF output, plus its engine's scratch (the segmented walk's samples,
-// memo tables, queues and key maps; the block and Jacobi copies).
-std::size_t EstimateBytes(const rdb_request& r) {
+// memo tables, queues and key maps; the block and Jacobi copies) and, when
+// its palette is built on the device, that build's classification scratch.
+std::size_t EstimateBytes(const rdb_request& r, bool device_palette) {
   const std::size_t px = static_cast<std::size_t>(r.width) * r.height;
+  std::size_t build = 0;
+  if (device_palette) {
+    const bool gray = rdb_is_grayscale(r.pixels, r.layout, static_cast<std::size_t>(r.width),
+                                       static_cast<std::size_t>(r.height), r.row_stride) != 0;
+    build = rdb::OctreeRowsScratch(static_cast<int64_t>(px),
+                                   TreeDepth(r.colors, r.associate_alpha != 0, gray),
+                                   r.associate_alpha != 0);
+  }
   std::size_t b = px * (rdb::BytesPerPixel(r.layout) + 1 + (r.rgba_out ? 16 : 0)) + 4 * px;
   if (r.engine == RDB_ENGINE_SEQ) {
     // Scratch and key maps; an alpha-associated palette also holds its
@@ -101,7 +123,7 @@ std::size_t EstimateBytes(const rdb_request& r) {
   } else {
     b += px * 24;
   }
-  return b + (std::size_t{1} << 20);
+  return b + build + (std::size_t{1} << 20);
 }
 
 bool SameOptions(const rdb_options& a, const rdb_options& b) {
@@ -218,9 +240,12 @@ void rdb_server::Work(int index) {
     const Clock::time_point t0 = Clock::now();
     std::vector<int> pids(batch.size(), 0);
     std::vector<rdb_host_job> jobs(batch.size());
+    std::vector<int> colors(batch.size()), assoc(batch.size());
+    std::vector<double> build_ms(batch.size(), 0.0);
+    const bool on_device = o.host_palettes == 0;
     int rc = crc;
     for (std::size_t i = 0; i < batch.size() && rc == RDB_OK; ++i) {
-      rc = rdb_palette_from_octree(ctx, batch[i]->tree, &pids[i]);
+      if (!on_device) rc = rdb_palette_from_octree(ctx, batch[i]->tree, &pids[i]);
       const rdb_request& r = batch[i]->r;
       rdb_host_job& j = jobs[i];
       j.pixels = r.pixels;
@@ -231,25 +256,48 @@ void rdb_server::Work(int index) {
       j.palette_id = pids[i];
       j.indices = r.indices;
       j.rgba_out = r.rgba_out;
+      colors[i] = r.colors;
+      assoc[i] = r.associate_alpha;
     }
     if (rc == RDB_OK) {
-      rc = rdb_dither_host(ctx, batch[0]->r.engine, jobs.data(), static_cast<int>(jobs.size()),
-                           &batch[0]->r.options);
+      if (on_device) {
+        rc = ctx->impl.DitherHostBuilding(batch[0]->r.engine, jobs.data(), colors.data(), assoc.data(),
+                                          static_cast<int>(jobs.size()), batch[0]->r.options,
+                                          build_ms.data());
+      } else {
+        rc = rdb_dither_host(ctx, batch[0]->r.engine, jobs.data(), static_cast<int>(jobs.size()),
+                             &batch[0]->r.options);
+      }
     }
     const std::string err = rc == RDB_OK ? std::string() : std::string(rdb_last_error());
     for (int pid : pids) {
       if (pid) rdb_palette_destroy(ctx, pid);
     }
     const Clock::time_point t1 = Clock::now();
+    // Built on the device: the builds ran one after another at the start of
+    // the batch call, then the walk.
+    Clock::time_point dither_start = t0;
+    if (on_device) {
+      double cum = 0.0;
+      for (std::size_t i = 0; i < batch.size(); ++i) {
+        const auto at = [&](double ms) {
+          return t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::milli>(ms));
+        };
+        batch[i]->t_build_start = at(cum);
+        cum += build_ms[i];
+        batch[i]->t_built = at(cum);
+      }
+      dither_start = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::milli>(cum));
+    }
     std::lock_guard<std::mutex> lk(mu);
     ++batches;
     for (Req* q : batch) {
       rdb_octree_free(q->tree);
       q->tree = nullptr;
       q->status = rc;
-      q->t_start = t0;
+      q->t_start = on_device ? dither_start : t0;
       q->t_done = t1;
-      q->device_ms = Ms(t0, t1);
+      q->device_ms = Ms(q->t_start, t1);
       q->batch = static_cast<int>(batch.size());
       q->err = err;
       q->done = true;
@@ -257,7 +305,7 @@ void rdb_server::Work(int index) {
       --pending;
       if (rc == RDB_OK) {
         latencies.push_back({Ms(q->t_submit, q->t_build_start), Ms(q->t_build_start, q->t_built),
-                             Ms(q->t_built, t0), Ms(t0, t1), Ms(q->t_submit, t1)});
+                             Ms(q->t_built, q->t_start), Ms(q->t_start, t1), Ms(q->t_submit, t1)});
         pixels += static_cast<int64_t>(q->r.width) * q->r.height;
         last_done = t1;
       } else {
@@ -288,7 +336,9 @@ int rdb_server_create(const rdb_server_options* opts, rdb_server** out) {
     return rdb::Fail(RDB_E_CUDA, "rdb_server_create: cudaMemGetInfo failed");
   }
   s->budget = s->o.memory_budget ? std::min(s->o.memory_budget, (free_b / 10) * 9) : (free_b / 10) * 9;
-  for (int i = 0; i < s->o.host_threads; ++i) s->builders.emplace_back([s] { s->Build(); });
+  if (s->o.host_palettes) {
+    for (int i = 0; i < s->o.host_threads; ++i) s->builders.emplace_back([s] { s->Build(); });
+  }
   for (int i = 0; i < s->o.workers; ++i) s->workers.emplace_back([s, i] { s->Work(i); });
   *out = s;
   return RDB_OK;
@@ -304,7 +354,7 @@ int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
   }
   Req* q = new Req();
   q->r = *req;
-  q->bytes = EstimateBytes(*req);
+  q->bytes = EstimateBytes(*req, s->o.host_palettes == 0);
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) {
     delete q;
@@ -321,10 +371,17 @@ int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
     s->first_submit = q->t_submit;
   }
   s->all[q->ticket] = q;
-  s->incoming.push_back(q);
   ++s->pending;
   *ticket = q->ticket;
-  s->cv_build.notify_one();
+  if (s->o.host_palettes) {
+    s->incoming.push_back(q);
+    s->cv_build.notify_one();
+  } else {
+    // Straight to admission: the device worker builds the palette.
+    q->t_build_start = q->t_built = q->t_submit;
+    s->ready.push_back(q);
+    s->cv_ready.notify_all();
+  }
   return RDB_OK;
 }
 

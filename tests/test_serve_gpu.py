@@ -1,7 +1,9 @@
 """The request loop (rdb_server_*): a mixed stream of sizes, palettes, layouts
 and engines submitted concurrently gives every request the same bytes as the
-same request alone; admission keeps within a tight budget; requests larger
-than the budget are refused at submission."""
+same request alone (its palette built by the host builder); admission keeps
+within a tight budget; requests larger than the budget are refused at
+submission.  Both palette paths: built on the device by the worker (the
+default) and by host threads (host_palettes)."""
 from __future__ import annotations
 
 import threading
@@ -38,9 +40,10 @@ def _alone(ctx, img, colors, engine, alpha):
         ctx.release_palette(pid)
 
 
-def test_mixed_stream_equals_each_request_alone(ctx):
+@pytest.mark.parametrize("host_palettes", [False, True])
+def test_mixed_stream_equals_each_request_alone(ctx, host_palettes):
     reqs = _mix(48, 3)
-    srv = sb.Server(workers=3, max_batch=16)
+    srv = sb.Server(workers=3, max_batch=16, host_palettes=host_palettes)
     try:
         tickets = [None] * len(reqs)
 
@@ -69,12 +72,14 @@ def test_mixed_stream_equals_each_request_alone(ctx):
         assert info["status"] == 0 and info["total_ms"] >= info["device_ms"]
 
 
-def test_admission_budget(ctx):
+@pytest.mark.parametrize("host_palettes", [False, True])
+def test_admission_budget(ctx, host_palettes):
     reqs = _mix(12, 7)
     # Room for roughly one mid-size request at a time: everything still
-    # completes, never more than the budget admitted at once.
-    budget = 96 << 20
-    srv = sb.Server(workers=2, budget=budget)
+    # completes, never more than the budget admitted at once.  (A palette built
+    # on the device counts its classification scratch too.)
+    budget = (96 if host_palettes else 256) << 20
+    srv = sb.Server(workers=2, budget=budget, host_palettes=host_palettes)
     try:
         tickets = [srv.submit(img, c, e, alpha=a) for img, c, e, a in reqs]
         outs = [srv.wait(t)[0] for t in tickets]
