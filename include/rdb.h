@@ -154,6 +154,8 @@ typedef struct rdb_kernel_stats {
   int64_t launches;        /* kernels the context launched for the sequential engine */
   int64_t seg_len;         /* segment length of the last segmented walk */
   int64_t chains;          /* segments (concurrent chains) of the last segmented walk */
+  int block_threads;       /* launch shape of the last block walk: threads per CTA ... */
+  int block_min_ctas;      /* ... and the CTAs per SM it was compiled for (the tuner's pick) */
 } rdb_kernel_stats;
 int rdb_context_profile(rdb_context* ctx, int enable);
 /* The block engine's index dump, the reference's `<prefix>.idx.bin`

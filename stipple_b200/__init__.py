@@ -35,7 +35,8 @@ class KernelStats(C.Structure):
     """rdb_kernel_stats (include/rdb.h)."""
     _fields_ = [("walk_launches", C.c_int64), ("walk_ms", C.c_double),
                 ("walk_positions", C.c_int64), ("passes", C.c_int64), ("launches", C.c_int64),
-                ("seg_len", C.c_int64), ("chains", C.c_int64)]
+                ("seg_len", C.c_int64), ("chains", C.c_int64), ("block_threads", C.c_int),
+                ("block_min_ctas", C.c_int)]
 
 
 class Options(C.Structure):

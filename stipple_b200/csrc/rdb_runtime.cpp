@@ -41,6 +41,14 @@ std::map<std::tuple<int, int, int>, SegTune>& SegTuneTable() {
   return table;
 }
 
+// The block walk's launch-shape table (BlockWalkShape), keyed by device,
+// alpha, float samples, log2 of the blocks and log2 of the padded block length;
+// shared by the process's contexts like the segment-length table.
+std::map<std::tuple<int, int, int, int, int>, SegTune>& ShapeTuneTable() {
+  static std::map<std::tuple<int, int, int, int, int>, SegTune> table;
+  return table;
+}
+
 std::size_t BytesPerPixel(int layout) { return layout == RDB_RGBAF32 ? 16 : static_cast<std::size_t>(layout); }
 
 void SetError(const std::string& msg) { g_error = msg; }
@@ -644,9 +652,62 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
   L.is_float = packed ? 0 : 1;
   scaled_weights(o.diffusion, L.sw);
   L.status = static_cast<int*>(status_.ptr);
+  // Launch shape: the fastest measured for this workload class; its first
+  // calls run each shape once, timed on the device (the very first untimed:
+  // it pays module loading and table builds).
+  int shape = 0, tune_slot = -1;
+  SegTune* tune = nullptr;
+  {
+    int lb = 0, lp = 0;
+    while ((int64_t{1} << (lb + 1)) <= blocks) ++lb;
+    while ((1 << (lp + 1)) <= bpad) ++lp;
+    std::lock_guard<std::mutex> lk(SegTuneLock());
+    tune = &ShapeTuneTable()[std::make_tuple(device_, L.assoc, L.is_float, lb, lp)];
+    if (tune->cand.empty()) {
+      for (int c = 0; c < kBlockWalkShapes; ++c) tune->cand.push_back(c);
+      tune->ms.assign(tune->cand.size(), -1.0);
+    }
+    if (!tune->warmed) {
+      if (sweeps <= 1) tune->warmed = true;
+    } else {
+      for (std::size_t c = 0; c < tune->cand.size() && tune_slot < 0; ++c) {
+        if (tune->ms[c] == -1.0) tune_slot = static_cast<int>(c);
+      }
+      if (sweeps > 1) tune_slot = -1;  // sweeps use what single walks measured
+      if (tune_slot >= 0) {
+        tune->ms[static_cast<std::size_t>(tune_slot)] = -2.0;
+        shape = tune->cand[static_cast<std::size_t>(tune_slot)];
+      } else {
+        int best = 0;
+        for (std::size_t c = 0; c < tune->cand.size(); ++c) {
+          if (tune->ms[c] >= 0 && (tune->ms[static_cast<std::size_t>(best)] < 0 ||
+                                   tune->ms[c] < tune->ms[static_cast<std::size_t>(best)])) {
+            best = static_cast<int>(c);
+          }
+        }
+        shape = tune->ms[static_cast<std::size_t>(best)] >= 0 ? tune->cand[static_cast<std::size_t>(best)] : 0;
+      }
+    }
+  }
+  BlockWalkShape(shape, L.assoc != 0, &stats_.block_threads, &stats_.block_min_ctas);
   if (sweeps <= 1) {
-    e = LaunchBlockWalk(L, positions, s);
-    if (e != cudaSuccess) return CudaFail(e, "blocks engine launch");
+    if ((e = LaunchBlockGather(L, s)) != cudaSuccess) return CudaFail(e, "blocks engine launch");
+    if (tune_slot >= 0) {
+      for (cudaEvent_t& ev : tune_ev_) {
+        if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return CudaFail(e, "tuner events");
+      }
+      cudaEventRecord(tune_ev_[0], s);
+    }
+    if ((e = LaunchBlockWalkOnly(L, s, shape)) != cudaSuccess) return CudaFail(e, "blocks engine launch");
+    if (tune_slot >= 0) {
+      float ms = 0.0f;
+      cudaEventRecord(tune_ev_[1], s);
+      cudaEventSynchronize(tune_ev_[1]);
+      std::lock_guard<std::mutex> lk(SegTuneLock());
+      tune->ms[static_cast<std::size_t>(tune_slot)] =
+          cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) == cudaSuccess ? ms : -1.0;
+    }
+    if ((e = LaunchBlockScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "blocks engine launch");
     if (!dump_prefix_.empty()) return DumpBlockIndices(L, positions, s);
     return RDB_OK;
   }
@@ -665,7 +726,7 @@ int Context::RunBlocks(int pid, int layout, std::vector<BlockImage>& all, const 
     L.q_out = qbuf[k & 1];
     L.changed = changed;
     if ((e = cudaMemsetAsync(changed, 0, sizeof(int), s)) != cudaSuccess ||
-        (e = LaunchBlockWalkOnly(L, s)) != cudaSuccess) {
+        (e = LaunchBlockWalkOnly(L, s, shape)) != cudaSuccess) {
       return CudaFail(e, "block sweep");
     }
     last_sweeps_ = k + 1;

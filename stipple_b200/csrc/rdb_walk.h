@@ -106,11 +106,16 @@ struct BlockLaunch {
   int* status;
 };
 
-cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream);
+// Launch shapes of the walk kernel (threads per CTA, CTAs per SM); results do
+// not depend on the shape.
+constexpr int kBlockWalkShapes = 4;
+void BlockWalkShape(int shape, bool assoc, int* threads, int* min_ctas);
+cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream,
+                            int shape = 0);
 // The three phases of LaunchBlockWalk separately (block sweeps walk many times
 // between one gather and one scatter).
 cudaError_t LaunchBlockGather(const BlockLaunch& L, cudaStream_t stream);
-cudaError_t LaunchBlockWalkOnly(const BlockLaunch& L, cudaStream_t stream);
+cudaError_t LaunchBlockWalkOnly(const BlockLaunch& L, cudaStream_t stream, int shape = 0);
 cudaError_t LaunchBlockScatter(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream);
 // The chosen index of every position of every image, in list order, images
 // back to back (`out`: total_positions bytes).

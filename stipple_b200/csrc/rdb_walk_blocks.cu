@@ -407,8 +407,11 @@ __device__ __forceinline__ void WalkBlock(const BlockLaunch& L, const tw::Plan& 
   }
   if (changed && L.changed) atomicAdd(L.changed, 1);
 }
-template <bool kAssoc, bool kFloat>
-__global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaunch L) {
+// kThreads per CTA (a multiple of 32: each warp is one group of 32 blocks)
+// and kMinCtas resident per SM -- the register budget -- are the launch shape
+// the tuner picks among (BlockWalkShape); every shape computes the same bytes.
+template <bool kAssoc, bool kFloat, int kThreads, int kMinCtas>
+__global__ void __launch_bounds__(kThreads, kMinCtas) BlockWalkKernel(BlockLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   {
     const int4* src = reinterpret_cast<const int4*>(L.plan);
@@ -424,13 +427,28 @@ __global__ void __launch_bounds__(128, kAssoc ? 3 : 4) BlockWalkKernel(BlockLaun
   WalkBlock<kAssoc, kFloat>(L, P, gb, r);
 }
 
-template <bool kAssoc, bool kFloat>
-cudaError_t LaunchWalk(const BlockLaunch& L, cudaStream_t stream) {
-  cudaError_t e = AllowMaxSmem(BlockWalkKernel<kAssoc, kFloat>);
+template <bool kAssoc, bool kFloat, int kThreads, int kMinCtas>
+cudaError_t LaunchShape(const BlockLaunch& L, cudaStream_t stream) {
+  cudaError_t e = AllowMaxSmem(BlockWalkKernel<kAssoc, kFloat, kThreads, kMinCtas>);
   if (e != cudaSuccess) return e;
-  const unsigned g2 = static_cast<unsigned>((L.total_blocks + 127) / 128);
-  BlockWalkKernel<kAssoc, kFloat><<<g2, 128, L.plan_smem, stream>>>(L);
+  const unsigned g2 = static_cast<unsigned>((L.total_blocks + kThreads - 1) / kThreads);
+  BlockWalkKernel<kAssoc, kFloat, kThreads, kMinCtas><<<g2, kThreads, L.plan_smem, stream>>>(L);
   return cudaGetLastError();
+}
+
+// The shapes: (threads, CTAs per SM) -- the same 128-register budget in three
+// CTA sizes, and a larger register budget (fewer resident warps, no spills).
+constexpr int kShapes[kBlockWalkShapes][2] = {{128, 4}, {256, 2}, {64, 8}, {128, 3}};
+
+template <bool kAssoc, bool kFloat>
+cudaError_t LaunchWalk(const BlockLaunch& L, int shape, cudaStream_t stream) {
+  // Alpha palettes carry a fourth channel: one CTA less per SM at each size.
+  switch (shape) {
+    case 1: return LaunchShape<kAssoc, kFloat, 256, kAssoc ? 1 : 2>(L, stream);
+    case 2: return LaunchShape<kAssoc, kFloat, 64, kAssoc ? 6 : 8>(L, stream);
+    case 3: return LaunchShape<kAssoc, kFloat, 128, kAssoc ? 2 : 3>(L, stream);
+    default: return LaunchShape<kAssoc, kFloat, 128, kAssoc ? 3 : 4>(L, stream);
+  }
 }
 // Owner-map scatter (src/rd_riemersma_cpu.cpp:698-710): position 0 is the
 // origin's first visit and the final position its last, so every position
@@ -547,10 +565,18 @@ cudaError_t LaunchBlockGather(const BlockLaunch& L, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-cudaError_t LaunchBlockWalkOnly(const BlockLaunch& L, cudaStream_t stream) {
+cudaError_t LaunchBlockWalkOnly(const BlockLaunch& L, cudaStream_t stream, int shape) {
   if (L.total_blocks <= 0) return cudaSuccess;
-  return L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, stream) : LaunchWalk<true, false>(L, stream))
-                 : (L.is_float ? LaunchWalk<false, true>(L, stream) : LaunchWalk<false, false>(L, stream));
+  if (shape < 0 || shape >= kBlockWalkShapes) shape = 0;
+  return L.assoc ? (L.is_float ? LaunchWalk<true, true>(L, shape, stream) : LaunchWalk<true, false>(L, shape, stream))
+                 : (L.is_float ? LaunchWalk<false, true>(L, shape, stream)
+                               : LaunchWalk<false, false>(L, shape, stream));
+}
+
+void BlockWalkShape(int shape, bool assoc, int* threads, int* min_ctas) {
+  if (shape < 0 || shape >= kBlockWalkShapes) shape = 0;
+  *threads = kShapes[shape][0];
+  *min_ctas = kShapes[shape][1] - (assoc ? (shape == 2 ? 2 : 1) : 0);
 }
 
 cudaError_t LaunchBlockScatter(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
@@ -559,11 +585,11 @@ cudaError_t LaunchBlockScatter(const BlockLaunch& L, int64_t total_positions, cu
   return cudaGetLastError();
 }
 
-cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream) {
+cudaError_t LaunchBlockWalk(const BlockLaunch& L, int64_t total_positions, cudaStream_t stream, int shape) {
   if (total_positions <= 0 || L.total_blocks <= 0) return cudaSuccess;
   cudaError_t e;
   if ((e = LaunchBlockGather(L, stream)) != cudaSuccess) return e;
-  if ((e = LaunchBlockWalkOnly(L, stream)) != cudaSuccess) return e;
+  if ((e = LaunchBlockWalkOnly(L, stream, shape)) != cudaSuccess) return e;
   return LaunchBlockScatter(L, total_positions, stream);
 }
 
