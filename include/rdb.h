@@ -269,7 +269,10 @@ typedef struct rdb_options {
                            with its memo table off); 1 = the point iteration with the
                            truncated inverse filter (jacobi_taps, jacobi_fp64), as the
                            reference's approx engine */
-  int reserved[2];
+  int seg_window;       /* segmented thread walk of ONE image: segments walked per pass beyond
+                           the verified front (0 = automatic: as many as the device holds
+                           resident at once; -1 = every unverified segment each pass) */
+  int reserved[1];
 } rdb_options;
 
 void rdb_options_default(rdb_options* o);

@@ -54,7 +54,8 @@ class Options(C.Structure):
         ("max_passes", C.c_int),
         ("loop_mode", C.c_int),
         ("jacobi_form", C.c_int),
-        ("reserved", C.c_int * 2),
+        ("seg_window", C.c_int),
+        ("reserved", C.c_int * 1),
     ]
 
 

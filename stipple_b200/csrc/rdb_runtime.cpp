@@ -1539,16 +1539,23 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   int seg_len = o.seg_len;
   SegTune* tune = nullptr;
   int tune_slot = -1;
+  const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0));
+  // One image walks a window of resident segments beyond its front each pass
+  // (rdb_tsw.h): segments can then be shorter than "all of them resident"
+  // allows -- a pass costs seg_len steps, and the front advances about as far
+  // per pass in positions, so shorter segments cost fewer steps in total.
+  const bool windowed = n == 1 && o.seg_window >= 0;
   if (seg_len <= 0) {
-    const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0));
     const int rule = static_cast<int>(std::min<int64_t>(16384, (all_px + resident - 1) / resident));
     int bucket = 0;
     while ((int64_t{1} << (bucket + 1)) <= all_px) ++bucket;
     std::lock_guard<std::mutex> lk(SegTuneLock());
-    tune = &SegTuneTable()[std::make_tuple(device_, bucket, assoc ? 1 : 0)];
+    tune = &SegTuneTable()[std::make_tuple(device_, bucket, (assoc ? 1 : 0) + (windowed ? 2 : 0))];
     if (tune->cand.empty()) {
-      for (int c : {rule, rule / 2, rule / 4, rule * 2}) {
-        c = std::min(16384, (std::max(c, 64) + 15) & ~15);
+      const std::initializer_list<int> all = {rule, rule / 2, rule / 4, rule * 2};
+      const std::initializer_list<int> win = {48, 32, 64, 96};
+      for (int c : windowed ? win : all) {
+        c = std::min(16384, (std::max(c, windowed ? 32 : 64) + 15) & ~15);
         if (std::find(tune->cand.begin(), tune->cand.end(), c) == tune->cand.end()) tune->cand.push_back(c);
       }
       tune->ms.assign(tune->cand.size(), -1.0);
@@ -1574,7 +1581,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       seg_len = tune->cand[static_cast<std::size_t>(best)];
     }
   }
-  seg_len = (std::max(seg_len, 64) + 15) & ~15;
+  seg_len = (std::max(seg_len, windowed ? 16 : 64) + 15) & ~15;
   for (int i = 0; i < n; ++i) {
     const rdb_job& j = jobs[i];
     const DevPlan* p = Plan(j.palette_id);
@@ -1638,7 +1645,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   if (int rc = Reserve(&tsw_q_, 3 * q_bytes, "segment queues")) return rc;
   if (int rc = Reserve(&tsw_cx_, static_cast<std::size_t>(positions) * (is_float ? 16 : 4), "gathered samples")) return rc;
   if (int rc = Reserve(&tsw_chosen_, static_cast<std::size_t>(positions), "segment indices")) return rc;
-  if (int rc = Reserve(&tsw_changed_, static_cast<std::size_t>(total), "segment queue flags")) return rc;
+  if (int rc = Reserve(&tsw_changed_, 4 * static_cast<std::size_t>(total), "segment flags")) return rc;
   if (use_cache) {
     if (int rc = Reserve(&tsw_own_, own_entries * sizeof(uint64_t), "segment memo tables")) return rc;
     if (int rc = Reserve(&tsw_list_, own_entries * sizeof(uint32_t), "segment memo lists")) return rc;
@@ -1693,6 +1700,15 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.bad[0] = bad;
   L.bad[1] = bad + n;
   L.changed = static_cast<uint8_t*>(tsw_changed_.ptr);
+  L.walked[0] = L.changed + total;
+  L.walked[1] = L.changed + 2 * static_cast<std::size_t>(total);
+  L.warmed = L.changed + 3 * static_cast<std::size_t>(total);
+  L.window = 0;
+  if (windowed) {
+    const int w = o.seg_window > 0 ? o.seg_window : static_cast<int>(std::min<int64_t>(resident, total));
+    if (w < total) L.window = std::max(1, w);
+  }
+  if (L.window > 0) cudaMemsetAsync(L.walked[0], 0, 2 * static_cast<std::size_t>(total), s);
   L.status = static_cast<int*>(status_.ptr);
   scaled_weights(o.diffusion, L.sw);
 
@@ -1849,9 +1865,12 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
         const TswImage& im = imgs[static_cast<std::size_t>(i)];
         const int f0 = std::max(front[static_cast<std::size_t>(i)], 0);
         if (f0 >= im.nsegs) continue;
-        stats_.walk_positions += im.n - static_cast<int64_t>(f0) * seg_len;
+        // Walked this pass: segments [f0, stop), plus the warm-ups of pass 0.
+        const int stop = L.window > 0 ? std::min(im.nsegs, f0 + L.window) : im.nsegs;
+        stats_.walk_positions += std::min<int64_t>(im.n, static_cast<int64_t>(stop) * seg_len) -
+                                 static_cast<int64_t>(f0) * seg_len;
         if (checked == 0) {
-          for (int kk = std::max(f0, 1); kk < im.nsegs; ++kk) {
+          for (int kk = std::max(f0, 1); kk < stop; ++kk) {
             stats_.walk_positions += std::min(kk * seg_len, warm_len);
           }
         }

@@ -8,6 +8,8 @@
 // queue instead of zeros) and the memo (rdb_tsw.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "rdb_device.cuh"
 #include "rdb_tsw.h"
 #include "rdb_uniform.h"
@@ -189,12 +191,15 @@ __device__ __forceinline__ int map_insert(uint32_t* keys, uint32_t mask, unsigne
 template <bool kFloat, bool kAssoc>
 __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& im,
                                             const tw::Plan& P, const double* errp, int k,
-                                            bool active, int lane) {
+                                            int front, bool active, int lane) {
   constexpr int C = kAssoc ? 4 : 3;
   const int sid = im.first_seg + k;
   const int begin = k * L.seg_len;
   const int end = active ? min(begin + L.seg_len, im.n) : begin;
-  const bool warmup = L.pass == 0 && k > 0;
+  // A warm-up start in pass 0, and in a window for a segment whose
+  // predecessor the previous pass did not walk (it entered the window).
+  const bool warmup = k > 0 && (L.pass == 0 ||
+                                (L.window > 0 && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
   const int ws = (active && warmup) ? begin - min(begin, L.warm_len) : begin;
   const int steps = end - ws;
   const int64_t base = im.cx_offset;
@@ -432,16 +437,30 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     }
   }
   if (active && memo) L.own_count[sid] = n_own;
-  if (active) L.changed[sid] = changed ? 1 : 0;
+  if (active) {
+    L.changed[sid] = changed ? 1 : 0;
+    if (L.window > 0) {
+      L.walked[L.pass & 1][sid] = 1;
+      L.warmed[sid] = warmup ? 1 : 0;
+    }
+  }
 }
 
 template <bool kFloat, bool kAssoc>
 __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const TswChunk ch = L.chunks[blockIdx.x];
+  int chunk = blockIdx.x;
+  if (L.window > 0) {
+    // One image: chunks are its segments 128 at a time; the grid covers the
+    // window, counted from the front's chunk.
+    chunk += front_of(L, 0, L.images[0].nsegs) / L.chunk_threads;
+    if (chunk >= L.n_chunks) return;
+  }
+  const TswChunk ch = L.chunks[chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
-  if (ch.k0 + ch.count <= front) return;  // the whole chunk is verified (uniform per CTA)
+  const int stop = L.window > 0 ? min(front + L.window, im.nsegs) : im.nsegs;
+  if (ch.k0 + ch.count <= front || ch.k0 >= stop) return;  // nothing to walk (uniform per CTA)
   {
     const int4* src = reinterpret_cast<const int4*>(im.plan);
     int4* dst = reinterpret_cast<int4*>(smem);
@@ -463,15 +482,16 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  // Warps whose segments are all verified or past the image leave together.
+  // Warps whose segments are all verified, past the window or past the image
+  // leave together.
   const int warp_k0 = ch.k0 + static_cast<int>(threadIdx.x & ~31u);
   const int warp_end = min(ch.k0 + ch.count, warp_k0 + 32);
-  if (warp_end <= front || warp_k0 >= ch.k0 + ch.count) return;
+  if (warp_end <= front || warp_k0 >= ch.k0 + ch.count || warp_k0 >= stop) return;
   const int k = ch.k0 + static_cast<int>(threadIdx.x);
-  const bool active = static_cast<int>(threadIdx.x) < ch.count && k >= front;
+  const bool active = static_cast<int>(threadIdx.x) < ch.count && k >= front && k < stop;
   tw::Plan P;
   P.bind(smem);
-  WalkSegment<kFloat, kAssoc>(L, im, P, errp, active ? k : warp_end - 1, active, lane);
+  WalkSegment<kFloat, kAssoc>(L, im, P, errp, active ? k : warp_end - 1, front, active, lane);
 }
 
 // G_new = the entries of G_prev that verified segments made; usemin cleared;
@@ -533,8 +553,9 @@ __global__ void TswVerifyKeys(TswLaunch L) {
 
 // The queue and own checks, one warp per walked segment.
 __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
-  const int sid_lo = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int sid_lo = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
+  if (L.window > 0) sid_lo += front_of(L, 0, L.images[0].nsegs);  // the grid covers the window
   if (sid_lo >= total_segs) return;
   const int sid = sid_lo;
   // Owner image of this global segment id.
@@ -548,6 +569,11 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
   if (k >= im.nsegs) return;
   const int front = front_of(L, lo, im.nsegs);
   if (k < front) return;  // verified earlier, not walked
+  if (L.window > 0 && k >= front + L.window) {
+    // Not walked this pass: the front stops at the window's end.
+    if (k == front + L.window && lane == 0) atomicMin(L.bad[L.pass & 1] + lo, k);
+    return;
+  }
   // Only the image's FIRST failure matters: segments past one already found
   // need no check.  (A relaxed read; a stale value only costs a check.)
   if (k > *reinterpret_cast<volatile const int*>(L.bad[L.pass & 1] + lo)) return;
@@ -555,11 +581,12 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
   if (k > front) {
     // The first walked segment started from a verified predecessor's queue;
     // the others from their predecessor's end queue of the previous pass,
-    // which the predecessor compared with its new one (L.changed).  Pass 0
-    // started from warm-ups and compares the queues themselves.
-    if (L.pass == 0) {
+    // which the predecessor compared with its new one (L.changed), or from a
+    // warm-up (pass 0, and segments entering a window), whose queue is
+    // compared with the predecessor's end queue itself.
+    if (L.pass == 0 || (L.window > 0 && L.warmed[sid])) {
       const double* a = L.q_start + static_cast<int64_t>(sid) * 64;
-      const double* b = L.q_end[0] + static_cast<int64_t>(sid - 1) * 64;
+      const double* b = L.q_end[L.pass & 1] + static_cast<int64_t>(sid - 1) * 64;
       for (int i = lane; i < 64; i += 32) {
         if (__double_as_longlong(a[i]) != __double_as_longlong(b[i])) ok = false;
       }
@@ -649,11 +676,24 @@ __global__ void TswControl(TswLaunch L, cudaGraphConditionalHandle handle, int* 
   *tag_dev += 1u;
 }
 
+// Grids: every chunk and every segment, or with a window the chunks and
+// segments it can reach from wherever the front is (one more chunk: the
+// window need not start on a chunk boundary; one more segment: the first one
+// past the window stops the front).
+unsigned TswWalkGrid(const TswLaunch& L) {
+  if (L.window <= 0) return static_cast<unsigned>(L.n_chunks);
+  return static_cast<unsigned>(std::min(L.n_chunks, (L.window + L.chunk_threads - 1) / L.chunk_threads + 1));
+}
+unsigned TswVerifyGrid(const TswLaunch& L, int total_segs) {
+  const int segs = L.window > 0 ? std::min(total_segs, L.window + 1) : total_segs;
+  return static_cast<unsigned>((segs + 7) / 8);
+}
+
 template <bool kFloat, bool kAssoc>
 cudaError_t LaunchWalk(const TswLaunch& L, int smem, cudaStream_t s) {
   const cudaError_t e = AllowMaxSmem(TswWalkKernel<kFloat, kAssoc>);
   if (e != cudaSuccess) return e;
-  TswWalkKernel<kFloat, kAssoc><<<L.n_chunks, L.chunk_threads, smem, s>>>(L);
+  TswWalkKernel<kFloat, kAssoc><<<TswWalkGrid(L), L.chunk_threads, smem, s>>>(L);
   return cudaGetLastError();
 }
 
@@ -706,7 +746,7 @@ cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) 
     }
   }
   if (total_segs <= 0) return cudaSuccess;
-  TswVerifySegments<<<(total_segs + 7) / 8, 256, 0, s>>>(L, total_segs);
+  TswVerifySegments<<<TswVerifyGrid(L, total_segs), 256, 0, s>>>(L, total_segs);
   return cudaGetLastError();
 }
 
@@ -758,7 +798,7 @@ cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int tota
   if (L->n_chunks > 0) {
     const void* wf = L->assoc ? (L->is_float ? WalkFunc<true, true>() : WalkFunc<false, true>())
                               : (L->is_float ? WalkFunc<true, false>() : WalkFunc<false, false>());
-    e = AddKernel(g, last, wf, dim3(L->n_chunks), dim3(L->chunk_threads),
+    e = AddKernel(g, last, wf, dim3(TswWalkGrid(*L)), dim3(L->chunk_threads),
                   static_cast<unsigned>(TswSmemBytes(L->plan_smem_max)), args1);
     if (e != cudaSuccess) return e;
   }
@@ -774,7 +814,7 @@ cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int tota
   }
   if (total_segs > 0) {
     void* args2[] = {L, &total_segs};
-    e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifySegments), dim3((total_segs + 7) / 8),
+    e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifySegments), dim3(TswVerifyGrid(*L, total_segs)),
                   dim3(256), 0, args2);
     if (e != cudaSuccess) return e;
   }

@@ -104,6 +104,16 @@ struct TswLaunch {
   // when the next segment, which started from that previous queue, started
   // from the wrong one.
   uint8_t* changed;
+  // Window (single-image launches; 0 = none): a pass walks only segments
+  // [front, front + window) of the image, so a whole wave of resident threads
+  // works at the front; the grids of the walk and of the segment checks cover
+  // the window only (chunk / segment ids counted from the front's chunk).  A
+  // segment whose predecessor the previous pass did not walk starts from a
+  // cache-free warm-up, as in pass 0 (walked[pass & 1] marks the walked ones,
+  // warmed[] the ones that started from a warm-up this pass).
+  int window;
+  uint8_t* walked[2];
+  uint8_t* warmed;
   int* status;
   // Device-side loop: the own-table tag of the running pass (null: use `tag`).
   const uint32_t* tag_dev;
