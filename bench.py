@@ -458,10 +458,10 @@ def run_ours(a, rank: int, world: int):
         chain["frame_frac"] = chain["frame_steps_per_s"] / bound
 
     # The same walk at 1920x1080 (the second frame size of the plain form).
-    fhd = bench_frame_size(ctx, s, a, 1920, 1080)
+    fhd = _side(bench_frame_size, ctx, s, a, 1920, 1080)
     # The call the reference's RiemersmaWalkCuda makes: RgbaF Q16 frame in a
     # host buffer, dithered in place (16 B/px each way), through the host C ABI.
-    rgbaf = bench_rgbaf_inplace(ctx, a, img, pid)
+    rgbaf = _side(bench_rgbaf_inplace, ctx, a, img, pid)
 
     out = {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
@@ -478,16 +478,28 @@ def run_ours(a, rank: int, world: int):
            "gpu_launches": int(kstats["launches"]) * a.steps}
 
     if rank == 0 and not a.skip_extra:
-        out["blocks"] = bench_blocks(ctx, s, a, tree, pid, hbm)
-        out["batched"] = bench_batched(ctx, s, a)
-        out["serve"] = bench_serve(ctx, a)
+        out["blocks"] = _side(bench_blocks, ctx, s, a, tree, pid, hbm)
+        out["batched"] = _side(bench_batched, ctx, s, a)
+        out["serve"] = _side(bench_serve, ctx, a)
     if rank == 0:
         cpu, _ = reference_cpu(img, C, budget_s=12.0)
         if not a.skip_extra:
-            cpu["all_cores"] = cpu_all_cores(a, img, C, [float(r) for r in a.serve_rates.split(",") if r])
+            cpu["all_cores"] = _side(cpu_all_cores, a, img, C,
+                                     [float(r) for r in a.serve_rates.split(",") if r])
         out["cpu_baseline"] = cpu
     ctx.release_palette(pid)
     return out
+
+
+def _side(fn, *args):
+    """A side measurement: its failure is recorded in the line (and its
+    traceback on stderr) instead of losing the headline."""
+    try:
+        return fn(*args)
+    except Exception as exc:  # noqa: BLE001 -- reported, not swallowed
+        import traceback
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{type(exc).__name__}: {exc}"}
 
 
 def bench_frame_size(ctx, s, a, W, H):

@@ -363,8 +363,12 @@ int rdb_dither_frames_host(rdb_context* ctx, const rdb_frames* f, const rdb_opti
  * A request loop over one device: requests of mixed sizes, palettes and
  * engines are submitted from any thread; host threads build each request's
  * palette (the library's octree, rdb_octree_build); requests are admitted
- * while the device-memory estimate of everything in flight stays within
- * `memory_budget`; idle device workers (each its own context and stream)
+ * while the device-memory bound of everything in flight, plus the buffers
+ * the workers' contexts keep between batches, stays within `memory_budget`
+ * (a context keeps at most an equal share of it; when a request cannot be
+ * admitted, idle contexts release theirs); idle device workers (each its own
+ * context and stream, held during a batch to what it had plus the batch's
+ * bound)
  * take every admitted request of one engine and one option set as one batch,
  * so requests that arrive while others are on the device join the next
  * batch and batches on different workers overlap.  Results are bit-identical
@@ -427,7 +431,8 @@ typedef struct rdb_server_stats {
   double p99_ms;
   double max_ms;
   double mpx_per_s;       /* pixels / (last completion - first submission) */
-  size_t peak_admitted_bytes;
+  size_t peak_admitted_bytes; /* most bytes counted against the budget at once
+                                 (admitted requests plus idle contexts' buffers) */
   double stage_p50_ms[RDB_STAGES]; /* per-stage percentiles (RDB_STAGE_*) */
   double stage_p99_ms[RDB_STAGES];
   int host_threads;       /* palette builders running */
@@ -435,6 +440,13 @@ typedef struct rdb_server_stats {
 } rdb_server_stats;
 
 int rdb_server_create(const rdb_server_options* opts, rdb_server** out);
+/* Device bytes the server counts for `req` while it is admitted (its staging,
+ * visit order, palette tables, the scratch of the engine path it takes and,
+ * unless host_palettes, its palette build's scratch): a request whose bytes
+ * exceed the server's budget is refused at submission.  Reads the pixels
+ * only to classify greyscale for a device palette build. */
+size_t rdb_request_bytes(const rdb_request* req, int host_palettes);
+
 /* Non-blocking; the request (and its buffers) must outlive its completion. */
 int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket);
 /* Waits up to timeout_ms (< 0 = forever) for one request; RDB_E_TIMEOUT when

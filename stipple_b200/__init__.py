@@ -176,6 +176,7 @@ SIGNATURES = {
     "rdb_context_last_sweeps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "rdb_server_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "rdb_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
+    "rdb_request_bytes": (C.c_size_t, [C.c_void_p, C.c_int]),
     "rdb_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p]),
     "rdb_server_stats_get": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rdb_server_stats_reset": (C.c_int, [C.c_void_p]),
@@ -676,8 +677,17 @@ class Server:
         _check(load().rdb_server_create(C.byref(o), C.byref(self.handle)))
         self._live: dict[int, tuple] = {}
 
-    def submit(self, img: np.ndarray, colors: int, engine: str | int = "seq",
-               alpha: bool = False, rgba: bool = False, **opts) -> int:
+    @staticmethod
+    def request_bytes(img: np.ndarray, colors: int, engine: str | int = "seq",
+                      alpha: bool = False, rgba: bool = False, host_palettes: bool = False,
+                      **opts) -> int:
+        """Device bytes a server counts for this request while admitted
+        (rdb_request_bytes)."""
+        img, r, _, _ = Server._request(img, colors, engine, alpha, rgba, opts)
+        return int(load().rdb_request_bytes(C.byref(r), int(host_palettes)))
+
+    @staticmethod
+    def _request(img, colors, engine, alpha, rgba, opts):
         # A crop of a larger image is submitted in place (its rows are
         # contiguous; the row stride says how far apart they are).
         if not (img.ndim == 3 and img.strides[2] == img.itemsize and
@@ -696,6 +706,11 @@ class Server:
         r.options = options(**opts)
         r.indices = _ptr(idx)
         r.rgba_out = _ptr(out) if out is not None else None
+        return img, r, idx, out
+
+    def submit(self, img: np.ndarray, colors: int, engine: str | int = "seq",
+               alpha: bool = False, rgba: bool = False, **opts) -> int:
+        img, r, idx, out = Server._request(img, colors, engine, alpha, rgba, opts)
         t = C.c_uint64()
         _check(load().rdb_server_submit(self.handle, C.byref(r), C.byref(t)))
         self._live[t.value] = (img, idx, out, r)

@@ -24,6 +24,8 @@ namespace {
 thread_local std::string g_error;
 
 constexpr std::size_t kMaxOrders = 1024;  // resident geometries before eviction
+constexpr std::size_t kOrderCacheBytes = std::size_t{1} << 30;  // and their bytes
+constexpr int kMaxAlphaSlabs = 64;  // plain walk: alpha memo slabs (32 MiB each) per launch
 
 std::size_t RowStride(const rdb_job& j) {
   return j.row_stride ? j.row_stride : static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
@@ -76,15 +78,10 @@ Context::~Context() {
     cudaFree(p.second.uniform);
   }
   for (auto& b : free_blocks_) cudaFree(b.second);
-  for (auto& o : orders_) cudaFree(o.second);
-  for (DevBuf* b : {&memo_, &memo_gen_, &seq_items_, &counter_, &status_, &curve_scratch_,
-                    &block_images_, &block_offsets_, &block_cx_, &block_chosen_, &jac_cx_,
-                    &jac_q_, &jac_g_, &host_in_, &host_idx_, &host_rgba_, &ssw_images_,
-                    &ssw_segs_, &ssw_work_, &ssw_q_, &ssw_ltab_, &ssw_g_, &ssw_bad_,
-                    &tsw_images_, &tsw_chunks_, &tsw_bad_, &tsw_q_, &tsw_own_, &tsw_list_,
-                    &tsw_count_, &tsw_cx_, &tsw_chosen_, &tsw_g_}) {
-    Release(b);
-  }
+  for (auto& o : orders_) cudaFree(o.second.dev);
+  for (DevBuf* b : CachedBufs()) Release(b);
+  Release(&counter_);
+  Release(&status_);
   for (cudaEvent_t& ev : ev_) {
     if (ev) cudaEventDestroy(ev);
   }
@@ -191,6 +188,61 @@ int Context::Init(int device, std::size_t budget) {
   return RDB_OK;
 }
 
+std::vector<DevBuf*> Context::CachedBufs() {
+  return {&memo_[0],     &memo_gen_[0],   &memo_[1],     &memo_gen_[1],   &seq_items_,   &curve_scratch_, &block_images_,
+          &block_offsets_, &block_cx_,    &block_chosen_, &jac_cx_,       &jac_q_,
+          &jac_g_,       &host_in_,       &host_idx_,    &host_rgba_,     &ssw_images_,
+          &ssw_segs_,    &ssw_work_,      &ssw_q_,       &ssw_ltab_,      &ssw_g_,
+          &ssw_bad_,     &tsw_images_,    &tsw_chunks_,  &tsw_bad_,       &tsw_q_,
+          &tsw_own_,     &tsw_list_,      &tsw_count_,   &tsw_cx_,        &tsw_chosen_,
+          &tsw_g_,       &dump_buf_,      &octree_scratch_, &tsw_changed_, &sweep_q_,
+          &octree_init_};
+}
+
+void Context::ReleaseScratch() {
+  cudaSetDevice(device_);
+  cudaStreamSynchronize(scratch_stream_ ? scratch_stream_ : stream_);
+  for (DevBuf* b : CachedBufs()) Release(b);
+  memo_grid_[0] = memo_grid_[1] = 0;
+  for (auto& o : orders_) {
+    cudaFree(o.second.dev);
+    bytes_ -= o.second.bytes;
+  }
+  orders_.clear();
+  order_bytes_ = 0;
+  for (auto& b : free_blocks_) {
+    cudaFree(b.second);
+    bytes_ -= b.first;
+  }
+  free_blocks_.clear();
+}
+
+bool Context::MakeRoom(std::size_t need) {
+  if (bytes_ + need <= budget_) return true;
+  // The device may still read what is freed here: wait for this context's
+  // work first.
+  cudaStreamSynchronize(scratch_stream_ ? scratch_stream_ : stream_);
+  for (auto& b : free_blocks_) {
+    cudaFree(b.second);
+    bytes_ -= b.first;
+  }
+  free_blocks_.clear();
+  while (bytes_ + need > budget_) {
+    auto victim = orders_.end();
+    for (auto it = orders_.begin(); it != orders_.end(); ++it) {
+      if (it->second.use != call_ && (victim == orders_.end() || it->second.use < victim->second.use)) {
+        victim = it;
+      }
+    }
+    if (victim == orders_.end()) return false;
+    cudaFree(victim->second.dev);
+    bytes_ -= victim->second.bytes;
+    order_bytes_ -= victim->second.bytes;
+    orders_.erase(victim);
+  }
+  return true;
+}
+
 void Context::Release(DevBuf* b) {
   if (b->ptr) {
     cudaFree(b->ptr);
@@ -205,7 +257,7 @@ int Context::Reserve(DevBuf* b, std::size_t bytes, const char* what) {
   // Grow geometrically so a stream of slightly larger jobs does not thrash.
   std::size_t want = std::max(bytes, b->bytes + b->bytes / 2);
   if (bytes_ - b->bytes + want > budget_) want = bytes;
-  if (bytes_ - b->bytes + want > budget_) {
+  if (bytes_ - b->bytes + want > budget_ && !MakeRoom(want - b->bytes)) {
     return Fail(RDB_E_NOMEM, std::string(what) + ": device memory budget exceeded");
   }
   if (b->ptr) {
@@ -230,7 +282,7 @@ void* Context::AllocBlock(std::size_t bytes, const char* what, int* rc) {
     *rc = RDB_OK;
     return p;
   }
-  if (bytes_ + bytes > budget_) {
+  if (bytes_ + bytes > budget_ && !MakeRoom(bytes)) {
     *rc = Fail(RDB_E_NOMEM, std::string(what) + ": budget exceeded");
     return nullptr;
   }
@@ -353,25 +405,32 @@ int Context::Order(int width, int height, cudaStream_t s, const int32_t** out) {
   const auto key = std::make_pair(width, height);
   auto it = orders_.find(key);
   if (it != orders_.end()) {
-    *out = it->second;
+    it->second.use = call_;
+    *out = it->second.dev;
     return RDB_OK;
   }
   const std::size_t n = static_cast<std::size_t>(width) * height;
   const std::size_t bytes = std::max<std::size_t>(n, 1) * sizeof(int32_t);
-  while ((orders_.size() >= kMaxOrders || bytes_ + bytes > budget_) && !order_lru_.empty()) {
-    // Evict the oldest geometry (after the device is done with it).
-    cudaDeviceSynchronize();
-    const auto victim = order_lru_.front();
-    order_lru_.erase(order_lru_.begin());
-    auto v = orders_.find(victim);
-    if (v != orders_.end()) {
-      cudaFree(v->second);
-      bytes_ -= std::max<std::size_t>(static_cast<std::size_t>(victim.first) * victim.second, 1) *
-                sizeof(int32_t);
-      orders_.erase(v);
+  // The cache keeps at most kMaxOrders geometries and kOrderCacheBytes:
+  // beyond either, least recently used orders the running call does not
+  // hold are evicted (after the device is done with them).
+  bool synced = false;
+  while (orders_.size() >= kMaxOrders || order_bytes_ + bytes > kOrderCacheBytes) {
+    auto victim = orders_.end();
+    for (auto v = orders_.begin(); v != orders_.end(); ++v) {
+      if (v->second.use != call_ && (victim == orders_.end() || v->second.use < victim->second.use)) victim = v;
     }
+    if (victim == orders_.end()) break;  // all held by this call: grow past the cap
+    if (!synced) {
+      cudaStreamSynchronize(scratch_stream_ ? scratch_stream_ : stream_);
+      synced = true;
+    }
+    cudaFree(victim->second.dev);
+    bytes_ -= victim->second.bytes;
+    order_bytes_ -= victim->second.bytes;
+    orders_.erase(victim);
   }
-  if (bytes_ + bytes > budget_) return Fail(RDB_E_NOMEM, "visit order: budget exceeded");
+  if (!MakeRoom(bytes)) return Fail(RDB_E_NOMEM, "visit order: budget exceeded");
   int32_t* d = nullptr;
   cudaError_t e = cudaMalloc(&d, bytes);
   if (e != cudaSuccess) return CudaFail(e, "visit order allocation");
@@ -389,8 +448,8 @@ int Context::Order(int width, int height, cudaStream_t s, const int32_t** out) {
     bytes_ -= bytes;
     return CudaFail(e, "visit order kernel");
   }
-  orders_[key] = d;
-  order_lru_.push_back(key);
+  orders_[key] = OrderEntry{d, bytes, call_};
+  order_bytes_ += bytes;
   *out = d;
   return RDB_OK;
 }
@@ -431,6 +490,7 @@ int Context::Dither(int engine, const rdb_job* jobs, int n, const rdb_options& o
   for (int i = 0; i < n; ++i) {
     if (int rc = CheckJob(jobs[i])) return rc;
   }
+  ++call_;
   if (!s) s = stream_;
   cudaSetDevice(device_);
   // The context's scratch buffers are shared by every call: a call on a new
@@ -497,8 +557,23 @@ int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t 
   const bool use_cache = o.use_cache != 0;
   // One warp per CTA.  Several CTAs share an SM once the batch is larger than
   // the SM count; shared memory is split between them.
-  const int per_sm = std::min(8, std::max(1, (n + sm_count_ - 1) / sm_count_));
-  const int grid = std::min(n, sm_count_ * per_sm);
+  int per_sm = std::min(8, std::max(1, (n + sm_count_ - 1) / sm_count_));
+  int grid = std::min(n, sm_count_ * per_sm);
+  // Memo slabs: one per CTA, 2^18 keys (2^24 with alpha), generation-tagged.
+  const int set = any_assoc ? 1 : 0;
+  const int64_t entries = any_assoc ? (int64_t{1} << 24) : (int64_t{1} << 18);
+  if (use_cache) {
+    // CTAs take images from the work counter, so fewer CTAs only walk more
+    // images each: an alpha slab is 32 MiB, so at most kMaxAlphaSlabs of
+    // them, and no more than half the budget left once the old slabs go.
+    const std::size_t slab = static_cast<std::size_t>(entries) * sizeof(uint16_t) + sizeof(uint32_t);
+    const std::size_t held = memo_[set].bytes + memo_gen_[set].bytes;
+    const std::size_t left = budget_ > bytes_ - held ? budget_ - (bytes_ - held) : 0;
+    int cap = static_cast<int>(std::min<std::size_t>(left / 2 / slab, 1 << 20));
+    if (any_assoc) cap = std::min(cap, kMaxAlphaSlabs);
+    grid = std::max(1, std::min(grid, std::max(cap, memo_grid_[set])));
+    per_sm = std::min(per_sm, std::max(1, (grid + sm_count_ - 1) / sm_count_));
+  }
   const std::size_t ring = 96 * (sizeof(int32_t) + 16);
   const std::size_t smem_cap = std::min<std::size_t>(smem_optin_, (228 * 1024) / per_sm - 1024);
   int cache_bits = o.cache_bits;
@@ -515,26 +590,19 @@ int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t 
   const std::size_t smem = SeqSmemBytes(plan_max, cache_bits, use_cache);
   if (smem > smem_optin_) return Fail(RDB_E_UNSUPPORTED, "palette plan does not fit in shared memory");
 
-  // Memo slabs: one per CTA, 2^18 keys (2^24 with alpha), generation-tagged.
-  const int64_t entries = any_assoc ? (int64_t{1} << 24) : (int64_t{1} << 18);
-  if (use_cache && (grid > memo_grid_ || entries > memo_entries_)) {
-    const int g = std::max(grid, memo_grid_);
-    const int64_t en = std::max(entries, memo_entries_);
+  if (use_cache && grid > memo_grid_[set]) {
     cudaDeviceSynchronize();  // earlier walks may still read the old slabs
-    Release(&memo_);
-    Release(&memo_gen_);
-    memo_grid_ = 0;
-    memo_entries_ = 0;
-    if (int rc = Reserve(&memo_, static_cast<std::size_t>(g) * en * sizeof(uint16_t), "memo slabs")) {
+    Release(&memo_[set]);
+    Release(&memo_gen_[set]);
+    memo_grid_[set] = 0;
+    const std::size_t g = static_cast<std::size_t>(grid);
+    if (int rc = Reserve(&memo_[set], g * static_cast<std::size_t>(entries) * sizeof(uint16_t), "memo slabs")) {
       return rc;
     }
-    if (int rc = Reserve(&memo_gen_, static_cast<std::size_t>(g) * sizeof(uint32_t), "memo generations")) {
-      return rc;
-    }
-    cudaMemsetAsync(memo_.ptr, 0, memo_.bytes, s);
-    cudaMemsetAsync(memo_gen_.ptr, 0, memo_gen_.bytes, s);
-    memo_grid_ = g;
-    memo_entries_ = en;
+    if (int rc = Reserve(&memo_gen_[set], g * sizeof(uint32_t), "memo generations")) return rc;
+    cudaMemsetAsync(memo_[set].ptr, 0, memo_[set].bytes, s);
+    cudaMemsetAsync(memo_gen_[set].ptr, 0, memo_gen_[set].bytes, s);
+    memo_grid_[set] = grid;
   }
   if (int rc = Reserve(&seq_items_, items.size() * sizeof(SeqItem), "work items")) return rc;
   cudaError_t e = cudaMemcpyAsync(seq_items_.ptr, items.data(), items.size() * sizeof(SeqItem),
@@ -548,9 +616,9 @@ int Context::Seq(const rdb_job* jobs, int n, const rdb_options& o, cudaStream_t 
   L.items = static_cast<const SeqItem*>(seq_items_.ptr);
   L.n_items = n;
   L.work_counter = static_cast<int*>(counter_.ptr);
-  L.memo = static_cast<uint16_t*>(memo_.ptr);
-  L.memo_gen = static_cast<uint32_t*>(memo_gen_.ptr);
-  L.slab_entries = memo_entries_;
+  L.memo = static_cast<uint16_t*>(memo_[set].ptr);
+  L.memo_gen = static_cast<uint32_t*>(memo_gen_[set].ptr);
+  L.slab_entries = entries;
   L.cache_bits = use_cache ? cache_bits : 0;
   L.plan_smem_max = plan_max;
   L.use_cache = use_cache ? 1 : 0;
@@ -964,6 +1032,7 @@ int Context::CheckFrames(const rdb_frames& f) const {
 
 int Context::Frames(const rdb_frames& f, const rdb_options& o, cudaStream_t s) {
   if (int rc = CheckFrames(f)) return rc;
+  ++call_;
   if (!s) s = stream_;
   cudaSetDevice(device_);
   if (!scratch_ev_) {
@@ -1910,6 +1979,79 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     stats_.chains = total;
   }
   return RDB_OK;
+}
+
+std::size_t ScratchBound(int engine, int width, int height, int layout, bool assoc, bool rgba_out,
+                         const rdb_options& o) {
+  using sz = std::size_t;
+  const sz n = static_cast<sz>(std::max(width, 1)) * static_cast<sz>(std::max(height, 1));
+  const bool is_float = layout == RDB_RGBAF32;
+  // Staging (StageHostJobs, 256-byte aligned slices), the visit order and its
+  // builder's scratch (Order), the palette's plan block (a shared-memory
+  // image, so below the opt-in limit, in 16 KiB classes) and uniform-key table.
+  sz b = n * BytesPerPixel(layout) + n + (rgba_out ? 16 * n : 0) + 3 * 256;
+  b += 4 * n + CurveScratchBytes(CurveLevel(width, height));
+  b += (sz{256} << 10) + (assoc ? sz{kUniformKeysAlpha} : sz{kUniformKeys});
+  const auto blocks = [&](sz block, bool sweeps) {
+    // RunBlocks: groups of 32 blocks of bpad <= block + 15 cells; the
+    // candidate table without alpha; the sweeps' two end-queue buffers.
+    const sz nb = (n + block - 1) / block;
+    const sz cells = (nb + 31) / 32 * 32 * (block + 15);
+    sz r = cells * ((is_float ? 16 : 4) + 1) + (assoc ? 0 : sz{kCandKeys} * 4) + 64 * nb;
+    if (sweeps) r += 2 * nb * 64 * sizeof(double) + 256;
+    return r;
+  };
+  if (engine == RDB_ENGINE_BLOCKS) return b + blocks(static_cast<sz>(std::max(o.block, 16)), false);
+  if (engine == RDB_ENGINE_JACOBI) {
+    if (o.jacobi_form == 0) return b + blocks(256, true);
+    const sz elem = o.jacobi_fp64 ? 8 : 4;
+    return b + n * 4 * elem + 2 * n + 64 + (static_cast<sz>(std::max(o.jacobi_taps, 0)) + 1) * 8;
+  }
+  const bool use_cache = o.use_cache != 0;
+  int mode = o.seq_mode;
+  if (mode == 0) mode = n < 8192 ? 1 : 3;  // SeqAuto's rule
+  if (mode == 1) {
+    // One memo slab (2^18 or 2^24 uint16 keys plus its generation) and a work
+    // item; the walk's CTAs never outnumber its images.
+    return b + (use_cache ? (assoc ? (sz{1} << 25) : (sz{1} << 19)) + 4 : 0) + 256;
+  }
+  if (mode == 2) {
+    // SeqSegmented: segments of [seg, 2 seg) positions, memo tables of fewer
+    // than 4 x 2 seg 8-byte entries, two queues each; first-touch maps.
+    const sz seg = static_cast<sz>(o.seg_len > 0 ? std::max(o.seg_len, 64) : 2048);
+    const sz segs = std::max<sz>(1, n / seg);
+    sz r = segs * (2 * 64 * sizeof(double) + 64) + 64;
+    if (use_cache) {
+      r += segs * 8 * 8 * seg;
+      sz cap = sz{1} << 18;
+      if (assoc) {
+        cap = 1024;
+        while (cap < std::min<sz>(2 * n, sz{1} << 25)) cap <<= 1;
+      }
+      r += cap * (assoc ? 16 : 8);
+    }
+    return b + r;
+  }
+  // SeqThreadSegmented: segments of at least 16 positions (32 when the tuner
+  // picks), three queue buffers and four flag bytes each; samples and
+  // indices; memo tables below 4 entries per position (16 at least per
+  // segment) of 8 + 4 bytes; first-touch maps (3 direct 2^18-word maps, or 5
+  // words per slot of a hashed map of 4n..8n slots).
+  const sz seg = static_cast<sz>(o.seg_len > 0 ? std::max(16, o.seg_len) : 32);
+  const sz segs = n / seg + 1;
+  sz r = (n + 16) * ((is_float ? 16 : 4) + 1) + segs * (3 * 64 * sizeof(double) + 4 + 4) +
+         (segs / 128 + 1) * sizeof(TswChunk) + sizeof(TswImage) + 64;
+  if (use_cache) {
+    r += (4 * (n + 16384) + 16 * segs) * 12 + 4 * segs;  // the last segment may be partial
+    if (assoc) {
+      sz cap = 4096;
+      while (cap < 4 * n && cap < (sz{1} << 25)) cap <<= 1;
+      r += 5 * cap * 4 + 16;
+    } else {
+      r += 3 * (sz{1} << 18) * 4;
+    }
+  }
+  return b + r;
 }
 
 }  // namespace rdb

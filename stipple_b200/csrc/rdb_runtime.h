@@ -37,6 +37,14 @@ int ReadPaletteText(const std::string& path, int expect_colors, std::vector<floa
                     int* count, bool* associate_alpha, bool* grayscale);
 int Fail(int code, const std::string& msg);
 int CudaFail(cudaError_t e, const char* what);
+
+// Upper bound of the device bytes one host image adds to a call of `engine`
+// on a context: its staging, its visit order, its palette's tables and the
+// scratch of the path the call takes for it (the segmented walk's samples,
+// queues, memo tables and key maps; the plain walk's memo slab; the block
+// copies).  The request loop admits by it.
+std::size_t ScratchBound(int engine, int width, int height, int layout, bool assoc, bool rgba_out,
+                         const rdb_options& o);
 std::string CudaErr(cudaError_t e, const char* what);
 
 // A device buffer that only grows.
@@ -112,6 +120,13 @@ class Context {
   int Synchronize(cudaStream_t s);
 
   std::size_t bytes() const { return bytes_; }
+  // The request loop's controls: the budget Reserve and the caches keep
+  // within, and the release of every cached buffer -- scratch, memo slabs,
+  // visit orders, idle palette blocks -- once the context's stream is done
+  // (resident palettes stay).
+  void SetBudget(std::size_t budget) { budget_ = budget; }
+  std::size_t budget() const { return budget_; }
+  void ReleaseScratch();
   cudaStream_t stream() const { return stream_; }
   int device() const { return device_; }
   int sm_count() const { return sm_count_; }
@@ -149,14 +164,30 @@ class Context {
   cudaStream_t stream_ = nullptr;
   int next_palette_ = 1;
   std::map<int, DevPlan> plans_;
-  std::map<std::pair<int, int>, int32_t*> orders_;
-  std::vector<std::pair<int, int>> order_lru_;
+  // Visit orders by geometry; `use` is the call that last asked for one, so
+  // an order the running call holds is never evicted under it.
+  struct OrderEntry {
+    int32_t* dev = nullptr;
+    std::size_t bytes = 0;
+    uint64_t use = 0;
+  };
+  std::map<std::pair<int, int>, OrderEntry> orders_;
+  std::size_t order_bytes_ = 0;
+  uint64_t call_ = 0;  // public calls so far (Dither, Frames)
+  // Frees least recently used orders the running call does not hold, and idle
+  // palette blocks, until `need` more bytes fit the budget; false if they
+  // cannot.
+  bool MakeRoom(std::size_t need);
+  // Every scratch buffer a call may grow (not the work counter, the status
+  // word or the pass-loop control words, which live as long as the context).
+  std::vector<DevBuf*> CachedBufs();
 
   // Sequential engine state.
-  DevBuf memo_;
-  DevBuf memo_gen_;
-  int memo_grid_ = 0;
-  int64_t memo_entries_ = 0;
+  // Plain-walk memo slabs, one set for RGB keys (2^18 per slab) and one for
+  // alpha keys (2^24), each grown to the most CTAs a call of its kind used.
+  DevBuf memo_[2];
+  DevBuf memo_gen_[2];
+  int memo_grid_[2] = {0, 0};
   DevBuf seq_items_;
   DevBuf counter_;
   DevBuf status_;

@@ -91,6 +91,10 @@ struct Req {
   std::string err;
 };
 
+// Device bytes an idle context keeps after releasing its buffers (its work
+// counter, status word and loop control words).
+constexpr std::size_t kContextFloor = 4096;
+
 // The octree build's classification depth (rd_octree.cpp:255-275).
 int TreeDepth(int colors, bool assoc, bool gray) {
   int depth = 1;
@@ -101,10 +105,10 @@ int TreeDepth(int colors, bool assoc, bool gray) {
   return std::min(8, std::max(2, depth));
 }
 
-// Device bytes one request needs while admitted: staging of input, indices and
-// RgbaF output, plus its engine's scratch (the segmented walk's samples,
-// memo tables, queues and key maps; the block and Jacobi copies) and, when
-// its palette is built on the device, that build's classification scratch.
+// Device bytes one request needs while admitted: the runtime's bound for its
+// engine and path (rdb::ScratchBound: staging, visit order, palette tables,
+// the walk's scratch) and, when its palette is built on the device, that
+// build's classification scratch.
 std::size_t EstimateBytes(const rdb_request& r, bool device_palette) {
   const std::size_t px = static_cast<std::size_t>(r.width) * r.height;
   std::size_t build = 0;
@@ -115,15 +119,9 @@ std::size_t EstimateBytes(const rdb_request& r, bool device_palette) {
                                    TreeDepth(r.colors, r.associate_alpha != 0, gray),
                                    r.associate_alpha != 0);
   }
-  std::size_t b = px * (rdb::BytesPerPixel(r.layout) + 1 + (r.rgba_out ? 16 : 0)) + 4 * px;
-  if (r.engine == RDB_ENGINE_SEQ) {
-    // Scratch and key maps; an alpha-associated palette also holds its
-    // 2^24-byte uniform-key table while the request is on the device.
-    b += px * 64 + (std::size_t{3} << 20) + (r.associate_alpha ? px * 16 + (std::size_t{1} << 24) : 0);
-  } else {
-    b += px * 24;
-  }
-  return b + build + (std::size_t{1} << 20);
+  return rdb::ScratchBound(r.engine, r.width, r.height, r.layout, r.associate_alpha != 0,
+                           r.rgba_out != nullptr, r.options) +
+         build + (std::size_t{1} << 20);
 }
 
 bool SameOptions(const rdb_options& a, const rdb_options& b) {
@@ -151,11 +149,40 @@ struct rdb_server {
   bool any = false;
   Clock::time_point first_submit, last_done;
   std::size_t peak = 0;
+  // Per worker: its context, the device bytes that context holds between
+  // batches (counted against the budget like admitted requests), and whether
+  // it is running a batch.
+  std::vector<rdb_context*> ctxs;
+  std::vector<std::size_t> cached;
+  std::vector<char> busy;
 
   void Build();
   void Work(int index);
   std::vector<Req*> TakeBatch();
+  std::size_t Held() const;
+  bool TrimIdle();
 };
+
+std::size_t rdb_server::Held() const {
+  std::size_t h = admitted;
+  for (std::size_t c : cached) h += c;
+  return h;
+}
+
+// Under the lock: idle workers' contexts release their cached buffers (the
+// workers wait on the lock, so nothing uses those contexts meanwhile).
+// False when none held anything to release.
+bool rdb_server::TrimIdle() {
+  bool any_freed = false;
+  for (std::size_t w = 0; w < ctxs.size(); ++w) {
+    if (!ctxs[w] || busy[w] || cached[w] == 0) continue;
+    const std::size_t before = ctxs[w]->impl.bytes();
+    ctxs[w]->impl.ReleaseScratch();
+    cached[w] = ctxs[w]->impl.bytes();
+    any_freed = any_freed || cached[w] < before;
+  }
+  return any_freed;
+}
 
 void rdb_server::Build() {
   for (;;) {
@@ -194,11 +221,17 @@ void rdb_server::Build() {
 std::vector<Req*> rdb_server::TakeBatch() {
   std::vector<Req*> batch;
   Req* head = nullptr;
-  for (Req* q : ready) {
-    if (admitted + q->bytes <= budget || admitted == 0) {
-      head = q;
-      break;
+  for (int attempt = 0; attempt < 2 && !head && !ready.empty(); ++attempt) {
+    for (Req* q : ready) {
+      if (Held() + q->bytes <= budget) {
+        head = q;
+        break;
+      }
     }
+    // Nothing fits: idle contexts give back their caches, then once more.
+    // With no batch running every context is idle, so the oldest request
+    // (never above the budget) then fits.
+    if (!head && !TrimIdle()) break;
   }
   if (!head) return batch;
   const int max_batch = o.max_batch > 0 ? o.max_batch : 512;
@@ -207,7 +240,7 @@ std::vector<Req*> rdb_server::TakeBatch() {
     const bool compatible = q == head ||
                             (q->r.engine == head->r.engine && SameOptions(q->r.options, head->r.options) &&
                              q->r.engine != RDB_ENGINE_BLOCKS);
-    if (compatible && (admitted + q->bytes <= budget || (admitted == 0 && q == head))) {
+    if (compatible && (q == head || Held() + q->bytes <= budget)) {
       admitted += q->bytes;
       batch.push_back(q);
       it = ready.erase(it);
@@ -215,16 +248,23 @@ std::vector<Req*> rdb_server::TakeBatch() {
       ++it;
     }
   }
-  peak = std::max(peak, admitted);
+  peak = std::max(peak, Held());
   return batch;
 }
 
 void rdb_server::Work(int index) {
   rdb_context* ctx = nullptr;
+  // Between batches a context keeps its buffers for the next one, up to an
+  // equal share of the budget; past that it releases them.
   const std::size_t share = budget / static_cast<std::size_t>(std::max(1, o.workers));
+  const std::size_t w = static_cast<std::size_t>(index);
   cudaSetDevice(o.device);
-  const int crc = rdb_context_create(o.device, share, &ctx);
-  (void)index;
+  const int crc = rdb_context_create(o.device, budget, &ctx);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    ctxs[w] = crc == RDB_OK ? ctx : nullptr;
+    cached[w] = crc == RDB_OK ? ctx->impl.bytes() : 0;
+  }
   for (;;) {
     std::vector<Req*> batch;
     {
@@ -236,6 +276,12 @@ void rdb_server::Work(int index) {
         return !batch.empty();
       });
       if (batch.empty()) break;
+      busy[w] = 1;
+      // The batch may hold what the context already has plus its admitted
+      // bytes, and no more.
+      std::size_t want = cached[w];
+      for (Req* q : batch) want += q->bytes;
+      if (crc == RDB_OK) ctx->impl.SetBudget(want);
     }
     const Clock::time_point t0 = Clock::now();
     std::vector<int> pids(batch.size(), 0);
@@ -274,6 +320,7 @@ void rdb_server::Work(int index) {
       if (pid) rdb_palette_destroy(ctx, pid);
     }
     const Clock::time_point t1 = Clock::now();
+    if (crc == RDB_OK && ctx->impl.bytes() > share) ctx->impl.ReleaseScratch();
     // Built on the device: the builds ran one after another at the start of
     // the batch call, then the walk.
     Clock::time_point dither_start = t0;
@@ -291,6 +338,8 @@ void rdb_server::Work(int index) {
     }
     std::lock_guard<std::mutex> lk(mu);
     ++batches;
+    busy[w] = 0;
+    cached[w] = crc == RDB_OK ? ctx->impl.bytes() : 0;
     for (Req* q : batch) {
       rdb_octree_free(q->tree);
       q->tree = nullptr;
@@ -314,6 +363,11 @@ void rdb_server::Work(int index) {
     }
     cv_done.notify_all();
     cv_ready.notify_all();  // memory freed: other workers may admit now
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    ctxs[w] = nullptr;
+    cached[w] = 0;
   }
   if (ctx) rdb_context_destroy(ctx);
 }
@@ -339,9 +393,17 @@ int rdb_server_create(const rdb_server_options* opts, rdb_server** out) {
   if (s->o.host_palettes) {
     for (int i = 0; i < s->o.host_threads; ++i) s->builders.emplace_back([s] { s->Build(); });
   }
+  s->ctxs.assign(static_cast<std::size_t>(s->o.workers), nullptr);
+  s->cached.assign(static_cast<std::size_t>(s->o.workers), 0);
+  s->busy.assign(static_cast<std::size_t>(s->o.workers), 0);
   for (int i = 0; i < s->o.workers; ++i) s->workers.emplace_back([s, i] { s->Work(i); });
   *out = s;
   return RDB_OK;
+}
+
+size_t rdb_request_bytes(const rdb_request* req, int host_palettes) {
+  if (!req || !req->pixels || req->width < 1 || req->height < 1) return 0;
+  return EstimateBytes(*req, host_palettes == 0);
 }
 
 int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
@@ -360,7 +422,7 @@ int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
     delete q;
     return rdb::Fail(RDB_E_INVALID, "rdb_server_submit: server is stopping");
   }
-  if (q->bytes > s->budget) {
+  if (q->bytes + static_cast<std::size_t>(s->o.workers) * kContextFloor > s->budget) {
     delete q;
     return rdb::Fail(RDB_E_NOMEM, "rdb_server_submit: request larger than the admission budget");
   }

@@ -75,20 +75,52 @@ def test_mixed_stream_equals_each_request_alone(ctx, host_palettes):
 @pytest.mark.parametrize("host_palettes", [False, True])
 def test_admission_budget(ctx, host_palettes):
     reqs = _mix(12, 7)
-    # Room for roughly one mid-size request at a time: everything still
-    # completes, never more than the budget admitted at once.  (A palette built
-    # on the device counts its classification scratch too.)
-    budget = (96 if host_palettes else 256) << 20
+    # Room for about two of the largest requests at once (rdb_request_bytes:
+    # the bound the server admits by), so requests wait for each other and
+    # idle workers release their cached buffers to let the next one in.
+    need = [sb.Server.request_bytes(img, c, e, alpha=a, host_palettes=host_palettes)
+            for img, c, e, a in reqs]
+    budget = 2 * max(need) + (1 << 20)
     srv = sb.Server(workers=2, budget=budget, host_palettes=host_palettes)
     try:
         tickets = [srv.submit(img, c, e, alpha=a) for img, c, e, a in reqs]
         outs = [srv.wait(t)[0] for t in tickets]
         st = srv.stats()
+        # Admitted bounds plus the contexts' kept buffers, never above it.
         assert st["peak_admitted_bytes"] <= budget
-        big = synth.gradient_rgb8(4096, 4096, 1)
+        assert st["completed"] == len(reqs) and st["failed"] == 0
+        big = synth.gradient_rgb8(2048, 2048, 1)
+        assert sb.Server.request_bytes(big, 16, "seq", host_palettes=host_palettes) > budget
         with pytest.raises(sb.RdbError):
             srv.submit(big, 16, "seq")
     finally:
         srv.close()
     for (img, c, e, a), idx in zip(reqs, outs):
         assert np.array_equal(idx, _alone(ctx, img, c, e, a)[0])
+
+
+def test_many_geometries_and_small_alpha_batches(ctx):
+    """More distinct image sizes than fit the workers' share of a small budget
+    (visit orders are evicted between calls, never under the call that holds
+    them), and batches of small alpha-associated images on the plain walk
+    (its memo slabs are 32 MiB each, capped per launch): all complete, equal
+    to each request alone."""
+    rng = np.random.default_rng(11)
+    reqs = []
+    for k in range(160):
+        w, h = int(rng.integers(8, 90)), int(rng.integers(8, 90))
+        alpha = k % 2 == 0
+        img = synth.gradient_rgba8(w, h, 900 + k) if alpha else synth.gradient_rgb8(w, h, 900 + k)
+        reqs.append((img, int(rng.choice([4, 16, 64])), alpha))
+    need = max(sb.Server.request_bytes(img, c, "seq", alpha=a) for img, c, a in reqs)
+    budget = 8 * need
+    srv = sb.Server(workers=2, budget=budget, max_batch=64)
+    try:
+        tickets = [srv.submit(img, c, "seq", alpha=a) for img, c, a in reqs]
+        outs = [srv.wait(t)[0] for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(reqs) and st["peak_admitted_bytes"] <= budget
+    for (img, c, a), idx in zip(reqs, outs):
+        assert np.array_equal(idx, _alone(ctx, img, c, "seq", a)[0])

@@ -191,3 +191,40 @@ def test_host_and_device_pass_loops_agree(ctx, oracle, alpha):
         assert np.array_equal(got, want)  # the context recovers after the error
     finally:
         ctx.release_palette(pid)
+
+
+@pytest.mark.parametrize("alpha", [False, True])
+@pytest.mark.parametrize("window,seg", [(1, 32), (5, 32), (37, 48), (130, 64)])
+def test_thread_segmented_window(ctx, oracle, alpha, window, seg):
+    """One image walked a window of segments beyond the front each pass:
+    segments entering the window start from warm-ups, the front stops at the
+    window's end; both pass loops, with and without the memo table."""
+    img = synth.gradient_rgba8(300, 170, 90) if alpha else synth.gradient_rgb8(300, 170, 90)
+    t = sb.Octree(img, 64, alpha)
+    pid = ctx.palette_from_octree(t)
+    q = synth.to_q16(img)
+    try:
+        for cache in (1, 0):
+            want, _, _ = oracle.walk_seq(q, 64, alpha, t.grayscale, use_cache=bool(cache))
+            for mode in (1, 2):
+                got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=seg, warm_len=16,
+                                      seg_window=window, use_cache=cache, loop_mode=mode)
+                assert np.array_equal(got, want), (cache, mode)
+                # The front advances at most a window per pass.
+                assert ctx.last_passes >= -(-(300 * 170) // (seg * window))
+    finally:
+        ctx.release_palette(pid)
+
+
+def test_thread_segmented_window_float(ctx, oracle):
+    rng = np.random.default_rng(6)
+    q = (rng.random((90, 140, 4)) * 65535.0).astype(np.float32)
+    tree = oracle.build_tree(q, 32, True, False)
+    pid = ctx.palette(tree.palette, tree.child, tree.color_number, tree.number_unique, True,
+                      parent=tree.parent)
+    try:
+        want, _, _ = oracle.walk_seq(q, 32, True, False)
+        got = ctx.dither_host("seq", q, pid, seq_mode=3, seg_len=32, warm_len=16, seg_window=9)
+        assert np.array_equal(got, want)
+    finally:
+        ctx.release_palette(pid)
