@@ -156,6 +156,9 @@ typedef struct rdb_kernel_stats {
   int64_t chains;          /* segments (concurrent chains) of the last segmented walk */
   int block_threads;       /* launch shape of the last block walk: threads per CTA ... */
   int block_min_ctas;      /* ... and the CTAs per SM it was compiled for (the tuner's pick) */
+  double octree_ms[4];     /* device palette builds (rdb_octree_build_device and the server's):
+                              host first loop, device classification with its transfers,
+                              host absorb, host reduction and colormap; summed, wall clock */
 } rdb_kernel_stats;
 int rdb_context_profile(rdb_context* ctx, int enable);
 /* The block engine's index dump, the reference's `<prefix>.idx.bin`
@@ -272,7 +275,13 @@ typedef struct rdb_options {
   int seg_window;       /* segmented thread walk of ONE image: segments walked per pass beyond
                            the verified front (0 = automatic: as many as the device holds
                            resident at once; -1 = every unverified segment each pass) */
-  int reserved[1];
+  int walk_form;        /* segmented thread walk: 1 = paired warps: per 32 segments a chain warp
+                           runs each step's dependent chain and a sum warp keeps the running
+                           sums of the pending pixels, handing each over through shared memory
+                           (a shorter step, fewer segments resident); 2 = one thread per
+                           segment doing both (more segments resident); 0 = automatic: paired
+                           for one image, whose walk is latency-bound, one thread per segment
+                           for several, whose walk is throughput-bound.  Same results. */
 } rdb_options;
 
 void rdb_options_default(rdb_options* o);

@@ -36,7 +36,7 @@ class KernelStats(C.Structure):
     _fields_ = [("walk_launches", C.c_int64), ("walk_ms", C.c_double),
                 ("walk_positions", C.c_int64), ("passes", C.c_int64), ("launches", C.c_int64),
                 ("seg_len", C.c_int64), ("chains", C.c_int64), ("block_threads", C.c_int),
-                ("block_min_ctas", C.c_int)]
+                ("block_min_ctas", C.c_int), ("octree_ms", C.c_double * 4)]
 
 
 class Options(C.Structure):
@@ -55,7 +55,7 @@ class Options(C.Structure):
         ("loop_mode", C.c_int),
         ("jacobi_form", C.c_int),
         ("seg_window", C.c_int),
-        ("reserved", C.c_int * 1),
+        ("walk_form", C.c_int),
     ]
 
 

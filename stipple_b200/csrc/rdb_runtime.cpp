@@ -856,7 +856,7 @@ int Context::JacobiSweeps(const rdb_job* jobs, int n, const rdb_options& o, cuda
 
 int Context::BuildOctree(const void* pixels, int layout, int width, int height, std::size_t stride,
                          int max_colors, bool assoc, bool gray, cudaStream_t s, Octree* out,
-                         int* device_rows) {
+                         int* device_rows, const void* host_pixels, std::size_t host_stride) {
   if (!s) s = stream_;
   cudaSetDevice(device_);
   *device_rows = 0;
@@ -867,13 +867,18 @@ int Context::BuildOctree(const void* pixels, int layout, int width, int height, 
   std::vector<float> widened(W * 4);
   cudaError_t fetch_error = cudaSuccess;
   const auto row_at = [&](std::size_t y) -> const float* {
-    const unsigned char* src = static_cast<const unsigned char*>(pixels) + y * stride;
-    const cudaError_t e = cudaMemcpyAsync(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) {
-      const cudaError_t e2 = cudaStreamSynchronize(s);
-      if (e2 != cudaSuccess) fetch_error = e2;
+    if (host_pixels) {
+      // The same rows in host memory: no copy back.
+      std::memcpy(raw.data(), static_cast<const unsigned char*>(host_pixels) + y * host_stride, raw.size());
     } else {
-      fetch_error = e;
+      const unsigned char* src = static_cast<const unsigned char*>(pixels) + y * stride;
+      const cudaError_t e = cudaMemcpyAsync(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) {
+        const cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e2 != cudaSuccess) fetch_error = e2;
+      } else {
+        fetch_error = e;
+      }
     }
     if (layout == RDB_RGBAF32) {
       std::memcpy(widened.data(), raw.data(), raw.size());
@@ -888,7 +893,16 @@ int Context::BuildOctree(const void* pixels, int layout, int width, int height, 
     return widened.data();
   };
   const std::size_t H = static_cast<std::size_t>(height);
+  using Clk = std::chrono::steady_clock;
+  Clk::time_point tick = Clk::now();
+  // Profiling: wall time of each part into stats_.octree_ms[part].
+  const auto lap = [&](int part) {
+    const Clk::time_point now = Clk::now();
+    if (profiling_) stats_.octree_ms[part] += std::chrono::duration<double, std::milli>(now - tick).count();
+    tick = now;
+  };
   const std::size_t y0 = out->Begin(row_at, W, H, max_colors, assoc, gray);
+  lap(0);
   if (fetch_error != cudaSuccess) return CudaFail(fetch_error, "octree row fetch");
   if (y0 < H) {
     // The first loop's live nodes, by key, to start the second from.
@@ -938,14 +952,17 @@ int Context::BuildOctree(const void* pixels, int layout, int width, int height, 
     if ((e = ClassifyRowsDevice(L, octree_scratch_.ptr, scratch, s, &rows)) != cudaSuccess) {
       return CudaFail(e, "octree classification");
     }
+    lap(1);
     if (out->Absorb(rows)) {
       *device_rows = static_cast<int>(H - y0);
     } else {
       out->ClassifyRows(row_at, W, y0, H);
       if (fetch_error != cudaSuccess) return CudaFail(fetch_error, "octree row fetch");
     }
+    lap(2);
   }
   out->Finish();
+  lap(3);
   return RDB_OK;
 }
 
@@ -1340,8 +1357,10 @@ int Context::DitherHostBuilding(int engine, const rdb_host_job* jobs, const int*
                                       static_cast<std::size_t>(j.height), j.row_stride);
     Octree tree;
     int rows = 0;
+    const std::size_t host_stride =
+        j.row_stride ? j.row_stride : static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
     int rc = BuildOctree(dj[i].pixels, j.layout, j.width, j.height, static_cast<std::size_t>(dj[i].row_stride),
-                         colors[i], assoc[i] != 0, gray != 0, stream_, &tree, &rows);
+                         colors[i], assoc[i] != 0, gray != 0, stream_, &tree, &rows, j.pixels, host_stride);
     int pid = 0;
     if (rc == RDB_OK) rc = CreatePaletteFromTree(tree, &pid);
     if (rc != RDB_OK) {
@@ -1547,6 +1566,7 @@ int Context::SeqSegmented(const rdb_job* jobs, int n, const rdb_options& o, cuda
     }
   }
   last_passes_ = pass;
+  loop_pending_ = false;  // this call's count, not an earlier device loop's
   if ((e = LaunchSswRgba(L, n, s)) != cudaSuccess) return CudaFail(e, "RgbaF output");
   return RDB_OK;
 }
@@ -1608,7 +1628,12 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   int seg_len = o.seg_len;
   SegTune* tune = nullptr;
   int tune_slot = -1;
-  const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0));
+  if (o.walk_form < 0 || o.walk_form > 2) return Fail(RDB_E_INVALID, "walk_form must be 0..2");
+  // Paired warps unless their shared memory (the plan, the residual-side
+  // colours and the mailboxes) leaves no room for a CTA.
+  bool paired = o.walk_form == 1 || (o.walk_form == 0 && n == 1);
+  if (paired && TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0, 1) <= 0) paired = false;
+  const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0, paired ? 1 : 0));
   // One image walks a window of resident segments beyond its front each pass
   // (rdb_tsw.h): segments can then be shorter than "all of them resident"
   // allows -- a pass costs seg_len steps, and the front advances about as far
@@ -1619,10 +1644,11 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     int bucket = 0;
     while ((int64_t{1} << (bucket + 1)) <= all_px) ++bucket;
     std::lock_guard<std::mutex> lk(SegTuneLock());
-    tune = &SegTuneTable()[std::make_tuple(device_, bucket, (assoc ? 1 : 0) + (windowed ? 2 : 0))];
+    tune = &SegTuneTable()[std::make_tuple(device_, bucket,
+                                           (assoc ? 1 : 0) + (windowed ? 2 : 0) + (paired ? 4 : 0))];
     if (tune->cand.empty()) {
       const std::initializer_list<int> all = {rule, rule / 2, rule / 4, rule * 2};
-      const std::initializer_list<int> win = {48, 32, 64, 96};
+      const std::initializer_list<int> win = {96, 64, 48, 128};
       for (int c : windowed ? win : all) {
         c = std::min(16384, (std::max(c, windowed ? 32 : 64) + 15) & ~15);
         if (std::find(tune->cand.begin(), tune->cand.end(), c) == tune->cand.end()) tune->cand.push_back(c);
@@ -1772,6 +1798,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.walked[0] = L.changed + total;
   L.walked[1] = L.changed + 2 * static_cast<std::size_t>(total);
   L.warmed = L.changed + 3 * static_cast<std::size_t>(total);
+  L.paired = paired ? 1 : 0;
   L.window = 0;
   if (windowed) {
     const int w = o.seg_window > 0 ? o.seg_window : static_cast<int>(std::min<int64_t>(resident, total));
@@ -1972,6 +1999,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
         cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]) == cudaSuccess ? ms : -1.0;
   }
   last_passes_ = pass + 1;
+  loop_pending_ = false;  // this call's count, not an earlier device loop's
   if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
   if (profiling_) {
     stats_.launches += 2;  // gather, scatter

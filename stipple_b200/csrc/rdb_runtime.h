@@ -98,10 +98,12 @@ class Context {
   // ColorTree::Build of an image in device memory (rdb_octree_build_device):
   // the first classification loop on the host over rows copied back, the
   // second on the device (rdb_octree_dev.cu), the reduction on the host.
-  // *device_rows receives how many rows the device classified.
+  // *device_rows receives how many rows the device classified.  When the
+  // caller still holds the image in host memory (host_pixels, host_stride),
+  // the first loop reads its rows there instead.
   int BuildOctree(const void* pixels, int layout, int width, int height, std::size_t row_stride,
                   int max_colors, bool assoc, bool gray, cudaStream_t s, Octree* out,
-                  int* device_rows);
+                  int* device_rows, const void* host_pixels = nullptr, std::size_t host_stride = 0);
 
   // Visit order of a geometry, built on first use and kept resident.
   int Order(int width, int height, cudaStream_t s, const int32_t** out);

@@ -101,6 +101,10 @@ __device__ __forceinline__ void sample(const TswLaunch& L, int64_t at, double (&
   }
 }
 
+// A compile-time slot of the 16-entry running-sum ring.
+template <int U>
+struct Step {};
+
 // Pixel t (slot U) takes its last term w15 * e_{t-1}: the head of a step,
 // the only part its colour lookup waits for.
 template <int U, int C>
@@ -125,6 +129,126 @@ __device__ __forceinline__ void RotateTail(const double (&sw)[16], double (&R)[1
   }
 #pragma unroll
   for (int c = 0; c < C; ++c) R[U][c] = p[c];
+}
+
+// The rotations at a compile-time slot (the unrolled loop) or at a run-time
+// one (a switch over the 16 slots).
+template <int C, int U>
+__device__ __forceinline__ void RotateHeadAt(Step<U>, const double (&sw)[16], const double (&R)[16][C],
+                                             const double (&e)[C], double (&v)[C]) {
+  RotateHead<U, C>(sw, R, e, v);
+}
+template <int C, int U>
+__device__ __forceinline__ void RotateTailAt(Step<U>, const double (&sw)[16], double (&R)[16][C],
+                                             const double (&e)[C], const double (&p)[C]) {
+  RotateTail<U, C>(sw, R, e, p);
+}
+#define RDB_SLOT_CASES(F) \
+  F(0) F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14)
+template <int C>
+__device__ __forceinline__ void RotateHeadAt(int u, const double (&sw)[16], const double (&R)[16][C],
+                                             const double (&e)[C], double (&v)[C]) {
+  switch (u) {
+#define RDB_CASE(n) \
+  case n: RotateHead<n, C>(sw, R, e, v); break;
+    RDB_SLOT_CASES(RDB_CASE)
+#undef RDB_CASE
+    default: RotateHead<15, C>(sw, R, e, v); break;
+  }
+}
+template <int C>
+__device__ __forceinline__ void RotateTailAt(int u, const double (&sw)[16], double (&R)[16][C],
+                                             const double (&e)[C], const double (&p)[C]) {
+  switch (u) {
+#define RDB_CASE(n) \
+  case n: RotateTail<n, C>(sw, R, e, p); break;
+    RDB_SLOT_CASES(RDB_CASE)
+#undef RDB_CASE
+    default: RotateTail<15, C>(sw, R, e, p); break;
+  }
+}
+// The ring slot after slot u, and a slot's sums read out.
+template <int U>
+__device__ __forceinline__ Step<(U + 1) & 15> next_slot(Step<U>) {
+  return {};
+}
+__device__ __forceinline__ int next_slot(int u) { return (u + 1) & 15; }
+template <int C, int U>
+__device__ __forceinline__ void RingAt(Step<U>, const double (&R)[16][C], double (&out)[C]) {
+#pragma unroll
+  for (int c = 0; c < C; ++c) out[c] = R[U][c];
+}
+template <int C>
+__device__ __forceinline__ void RingAt(int u, const double (&R)[16][C], double (&out)[C]) {
+  switch (u) {
+#define RDB_CASE(n)                              \
+  case n:                                        \
+    for (int c = 0; c < C; ++c) out[c] = R[n][c]; \
+    break;
+    RDB_SLOT_CASES(RDB_CASE)
+#undef RDB_CASE
+    default:
+      for (int c = 0; c < C; ++c) out[c] = R[15][c];
+      break;
+  }
+}
+#undef RDB_SLOT_CASES
+
+// ---- paired walkers: the exchange ------------------------------------------
+// In the paired form two warps of a CTA walk the same 32 segments: the chain
+// warp runs each step's dependent chain (head, target, key, lookups, index,
+// residual), the sum warp the rest of the step (the 15 pending pixels taking
+// the new residual, the ring slot refilled with the next sample).  Per step
+// the sum warp hands over pixel t's running sum and the chain warp hands back
+// its residual, each through one of two mailboxes chosen by step parity, each
+// mailbox guarded by an mbarrier that all 32 lanes of the writing warp arrive
+// on.  A side can be at most one phase ahead on either barrier: the sum for
+// step i + 2 needs the residual of step i, and the residual of step i + 2
+// needs the sum for step i + 2.
+struct PairBox {
+  double s[2][4][32];   // running sums by step parity, channel-planar
+  double e[2][4][32];   // residuals by step parity
+  uint64_t full_s[2];   // sum warp -> chain warp
+  uint64_t full_e[2];   // chain warp -> sum warp
+};
+constexpr int kPairsPerCta = 4;  // 8 warps: 4 chain warps, then their 4 sum warps
+constexpr int kPairCtaThreads = 64 * kPairsPerCta;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void pair_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(32) : "memory");
+}
+__device__ __forceinline__ void pair_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+// Waits for the phase of parity `parity` to complete.  Bounded: after about a
+// second of clock cycles it sets the status word and returns false, so a
+// partner that never arrives ends the launch with an error, never a hang.
+__device__ __forceinline__ bool pair_wait(uint64_t* bar, unsigned parity, int* status) {
+  const unsigned addr = smem_u32(bar);
+  long long start = 0;
+#pragma unroll 1
+  for (unsigned it = 0;; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it == 0) start = clock64();
+    if ((it & 63u) == 63u && clock64() - start > (1ll << 31)) {
+      atomicExch(status, kDevTimeout);
+      return false;
+    }
+  }
 }
 
 __device__ __forceinline__ unsigned own_hash(unsigned key) { return (key * 0x9E3779B1u) >> 8; }
@@ -188,19 +312,28 @@ __device__ __forceinline__ int map_insert(uint32_t* keys, uint32_t mask, unsigne
 // serially in one lane while the other 31 wait.  kAssoc: the palette
 // associates alpha (four channels, 24-bit keys in hashed maps, no
 // uniform-key table); otherwise three channels and direct 2^18-key maps.
-template <bool kFloat, bool kAssoc>
+template <bool kFloat, bool kAssoc, bool kChain>
 __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& im,
                                             const tw::Plan& P, const double* errp, int k,
-                                            int front, bool active, int lane) {
+                                            int front, bool active, int lane, PairBox* box) {
   constexpr int C = kAssoc ? 4 : 3;
   const int sid = im.first_seg + k;
   const int begin = k * L.seg_len;
   const int end = active ? min(begin + L.seg_len, im.n) : begin;
-  // A warm-up start in pass 0, and in a window for a segment whose
-  // predecessor the previous pass did not walk (it entered the window).
+  // A cache-free start in pass 0 (after warm_len warm-up positions), and in
+  // a window for a segment whose predecessor the previous pass did not walk
+  // (it entered the window): that one starts from an empty queue with no
+  // warm-up -- it lies far past the front, and a warm-up would hold up the
+  // whole launch while buying almost no progress.
   const bool warmup = k > 0 && (L.pass == 0 ||
                                 (L.window > 0 && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
-  const int ws = (active && warmup) ? begin - min(begin, L.warm_len) : begin;
+  const int ws = (active && warmup) ? begin - min(begin, L.pass == 0 ? L.warm_len : 0) : begin;
+  if (active && warmup && ws == begin) {
+    // No warm-up position writes the start queue: it is the empty one.
+    double* qs0 = L.q_start + static_cast<int64_t>(sid) * 64;
+#pragma unroll 4
+    for (int i = 0; i < 64; ++i) qs0[i] = 0.0;
+  }
   const int steps = end - ws;
   const int64_t base = im.cx_offset;
   const bool memo = L.use_cache != 0;
@@ -209,6 +342,16 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   double e[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) e[c] = 0.0;
+  if constexpr (kChain) {
+    // The sum warp holds the ring; the chain warp only needs the pending
+    // residual q[15] of the predecessor's end queue.
+    (void)R;
+    if (active && !warmup && k > 0) {
+      const double* q = L.q_end[(L.pass & 1) ^ 1] + static_cast<int64_t>(sid - 1) * 64;
+#pragma unroll
+      for (int c = 0; c < C; ++c) e[c] = q[60 + c];
+    }
+  } else {
 #pragma unroll
   for (int u = 0; u < 16; ++u) {
     double p[C];
@@ -237,6 +380,7 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
 #pragma unroll
     for (int c = 0; c < C; ++c) e[c] = q[60 + c];
   }
+  }
 
   const uint32_t* gprev = im.g[(L.pass & 1) ^ 1];
   uint32_t* gnew = im.g[L.pass & 1];
@@ -256,185 +400,184 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   bool changed = false;
   int n_own = 0;
   uint32_t acc = 0;
-#pragma unroll 1
-  for (int i = 0; i < warp_steps; ++i) {
-    const bool on = i < steps;
-    const int t = ws + i;
-    const int u = i & 15;
-    float f[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    unsigned br = 0, bg = 0, bb = 0, ba = 0, key = 0, h = 0;
-    int index = 0, slot = 0;
-    bool search = false, record = false, from_g = false, booked = false, present = true;
-    const bool live = t >= begin;
-    const bool keyed = on && memo && live;
-    if (on) {
-      double p[C];
+  // One step of the walk; U = the step index mod 16 is a compile-time
+  // constant, so the running sums stay in fixed registers with no
+  // indexed jump per step.
+  const auto step = [&](auto u, const int i) -> bool {
+      if constexpr (kChain) {
+        // Pixel t's running sum from the sum warp (every lane waits).
+        if (!pair_wait(&box->full_s[i & 1], (i >> 1) & 1, L.status)) return false;
+      }
+      const bool on = i < steps;
+      const int t = ws + i;
+      float f[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      unsigned br = 0, bg = 0, bb = 0, ba = 0, key = 0, h = 0;
+      int index = 0, slot = 0;
+      bool search = false, record = false, from_g = false, booked = false, present = true;
+      (void)present;  // hashed maps only
+      const bool live = t >= begin;
+      const bool keyed = on && memo && live;
+      if (on) {
+        double p[C];
 #pragma unroll
-      for (int c = 0; c < C; ++c) p[c] = 0.0;
-      if (t + 16 < end) sample<kFloat, C>(L, base + t + 16, p);
-      double v[C];
-      switch (u) {
-        case 0: RotateHead<0, C>(L.sw, R, e, v); break;
-        case 1: RotateHead<1, C>(L.sw, R, e, v); break;
-        case 2: RotateHead<2, C>(L.sw, R, e, v); break;
-        case 3: RotateHead<3, C>(L.sw, R, e, v); break;
-        case 4: RotateHead<4, C>(L.sw, R, e, v); break;
-        case 5: RotateHead<5, C>(L.sw, R, e, v); break;
-        case 6: RotateHead<6, C>(L.sw, R, e, v); break;
-        case 7: RotateHead<7, C>(L.sw, R, e, v); break;
-        case 8: RotateHead<8, C>(L.sw, R, e, v); break;
-        case 9: RotateHead<9, C>(L.sw, R, e, v); break;
-        case 10: RotateHead<10, C>(L.sw, R, e, v); break;
-        case 11: RotateHead<11, C>(L.sw, R, e, v); break;
-        case 12: RotateHead<12, C>(L.sw, R, e, v); break;
-        case 13: RotateHead<13, C>(L.sw, R, e, v); break;
-        case 14: RotateHead<14, C>(L.sw, R, e, v); break;
-        default: RotateHead<15, C>(L.sw, R, e, v); break;
-      }
+        for (int c = 0; c < C; ++c) p[c] = 0.0;
+        double v[C];
+        if constexpr (kChain) {
+          (void)p;
 #pragma unroll
-      for (int c = 0; c < C; ++c) f[c] = clamp_pixel(v[c]);
-      br = byte_dev(f[0]);
-      bg = byte_dev(f[1]);
-      bb = byte_dev(f[2]);
-      key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12);
-      if constexpr (kAssoc) {
-        ba = byte_dev(f[3]);
-        key |= (ba >> 2) << 18;
-      }
-      // A uniform key's search result (and so its memo value) is fixed by the
-      // key: no search, no memo, no bookkeeping.
-      uint8_t uv = kNotUniform;
-      uint32_t gv = kNone;
-      if constexpr (kAssoc) {
-        // Keys the table has classified uniform need no memo; keys not yet
-        // classified, and the rest, go through the hashed map.
-        if (uni) {
-          uv = __ldg(uni + key);
-          if (uv == kUniformUnknown) uv = kNotUniform;
-        }
-        if (keyed && uv == kNotUniform) {
-          slot = map_find(hkeys, hmask, key, &present);
-          if (present) gv = __ldg(gprev + slot);
-        }
-      } else {
-        uv = __ldg(uni + key);
-        slot = static_cast<int>(key);
-        if (keyed) gv = __ldg(gprev + key);  // both loads in flight together
-      }
-      switch (u) {
-        case 0: RotateTail<0, C>(L.sw, R, e, p); break;
-        case 1: RotateTail<1, C>(L.sw, R, e, p); break;
-        case 2: RotateTail<2, C>(L.sw, R, e, p); break;
-        case 3: RotateTail<3, C>(L.sw, R, e, p); break;
-        case 4: RotateTail<4, C>(L.sw, R, e, p); break;
-        case 5: RotateTail<5, C>(L.sw, R, e, p); break;
-        case 6: RotateTail<6, C>(L.sw, R, e, p); break;
-        case 7: RotateTail<7, C>(L.sw, R, e, p); break;
-        case 8: RotateTail<8, C>(L.sw, R, e, p); break;
-        case 9: RotateTail<9, C>(L.sw, R, e, p); break;
-        case 10: RotateTail<10, C>(L.sw, R, e, p); break;
-        case 11: RotateTail<11, C>(L.sw, R, e, p); break;
-        case 12: RotateTail<12, C>(L.sw, R, e, p); break;
-        case 13: RotateTail<13, C>(L.sw, R, e, p); break;
-        case 14: RotateTail<14, C>(L.sw, R, e, p); break;
-        default: RotateTail<15, C>(L.sw, R, e, p); break;
-      }
-      search = uv == kNotUniform;
-      index = uv;
-      booked = keyed && search;
-      if (booked) {
-        if (gv != kNone && static_cast<int>(gv >> 8) < k) {
-          index = static_cast<int>(gv & 0xFFu);
-          search = false;
-          from_g = true;
+          for (int c = 0; c < C; ++c) v[c] = __dadd_rn(box->s[i & 1][c][lane], __dmul_rn(L.sw[15], e[c]));
         } else {
-          h = own_hash(key) & omask;
-          bool placed = false;
+          if (t + 16 < end) sample<kFloat, C>(L, base + t + 16, p);
+          RotateHeadAt<C>(u, L.sw, R, e, v);
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) f[c] = clamp_pixel(v[c]);
+        br = byte_dev(f[0]);
+        bg = byte_dev(f[1]);
+        bb = byte_dev(f[2]);
+        key = (br >> 2) | ((bg >> 2) << 6) | ((bb >> 2) << 12);
+        if constexpr (kAssoc) {
+          ba = byte_dev(f[3]);
+          key |= (ba >> 2) << 18;
+        }
+        // A uniform key's search result (and so its memo value) is fixed by the
+        // key: no search, no memo, no bookkeeping.
+        uint8_t uv = kNotUniform;
+        uint32_t gv = kNone;
+        if constexpr (kAssoc) {
+          // Keys the table has classified uniform need no memo; keys not yet
+          // classified, and the rest, go through the hashed map.
+          if (uni) {
+            uv = __ldg(uni + key);
+            if (uv == kUniformUnknown) uv = kNotUniform;
+          }
+          if (keyed && uv == kNotUniform) {
+            slot = map_find(hkeys, hmask, key, &present);
+            if (present) gv = __ldg(gprev + slot);
+          }
+        } else {
+          uv = __ldg(uni + key);
+          slot = static_cast<int>(key);
+          if (keyed) gv = __ldg(gprev + key);  // both loads in flight together
+        }
+        if constexpr (!kChain) RotateTailAt<C>(u, L.sw, R, e, p);
+        search = uv == kNotUniform;
+        index = uv;
+        booked = keyed && search;
+        if (booked) {
+          if (gv != kNone && static_cast<int>(gv >> 8) < k) {
+            index = static_cast<int>(gv & 0xFFu);
+            search = false;
+            from_g = true;
+          } else {
+            h = own_hash(key) & omask;
+            bool placed = false;
 #pragma unroll 1
-          for (unsigned probe = 0; probe <= omask; ++probe) {
-            const uint64_t ent = ot[h];
-            if ((ent & 0xFFFFFFFF00000000ull) != tag) {
-              placed = true;  // free slot for this pass: first own use of the key
-              break;
+            for (unsigned probe = 0; probe <= omask; ++probe) {
+              const uint64_t ent = ot[h];
+              if ((ent & 0xFFFFFFFF00000000ull) != tag) {
+                placed = true;  // free slot for this pass: first own use of the key
+                break;
+              }
+              if ((ent & 0xFFFFFFu) == key) {
+                index = static_cast<int>((ent >> 24) & 0xFFu);
+                search = false;
+                break;
+              }
+              h = (h + 1u) & omask;
             }
-            if ((ent & 0xFFFFFFu) == key) {
-              index = static_cast<int>((ent >> 24) & 0xFFu);
-              search = false;
-              break;
-            }
-            h = (h + 1u) & omask;
-          }
-          if (search) {
-            if (placed) {
-              record = true;
-            } else {
-              atomicExch(L.status, kDevBadPlan);  // table full: the host sizes it to 2x a segment
+            if (search) {
+              if (placed) {
+                record = true;
+              } else {
+                atomicExch(L.status, kDevBadPlan);  // table full: the host sizes it to 2x a segment
+              }
             }
           }
         }
       }
-    }
-    // The warp's searches, one target at a time over all 32 lanes.
-    unsigned want = __ballot_sync(0xffffffffu, search);
-    const int node = search ? tw::descend<kAssoc>(P, br, bg, bb, ba) : 0;
+      // The warp's searches, one target at a time over all 32 lanes.
+      unsigned want = __ballot_sync(0xffffffffu, search);
+      const int node = search ? tw::descend<kAssoc>(P, br, bg, bb, ba) : 0;
 #pragma unroll 1
-    while (want) {
-      const int src = __ffs(want) - 1;
-      want &= want - 1u;
-      const int sn = __shfl_sync(0xffffffffu, node, src);
-      double t4[4];
+      while (want) {
+        const int src = __ffs(want) - 1;
+        want &= want - 1u;
+        const int sn = __shfl_sync(0xffffffffu, node, src);
+        double t4[4];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) t4[c] = static_cast<double>(__shfl_sync(0xffffffffu, f[c], src));
-      if constexpr (kAssoc) {
-        // ClosestColor's target: beta * t with beta = QS * t.a (rd_octree.cpp:190-208).
-        const double beta = __dmul_rn(kQuantumScale, t4[3]);
-        t4[0] = __dmul_rn(beta, t4[0]);
-        t4[1] = __dmul_rn(beta, t4[1]);
-        t4[2] = __dmul_rn(beta, t4[2]);
-      }
-      const int r = tw::search_warp<kAssoc>(P, sn, t4[0], t4[1], t4[2], t4[3], lane);
-      if (lane == src) index = r;
-    }
-    if (booked) {
-      if constexpr (kAssoc) {
-        if (!present) slot = map_insert(hkeys, hmask, key, slot, im.hlist, im.hcount);
-        if (slot < 0) atomicExch(L.status, kDevBadPlan);  // key map full: cannot happen at its size
-      }
-      if (slot >= 0) red_min(gnew + slot, (static_cast<uint32_t>(k) << 8) | static_cast<uint32_t>(index));
-    }
-    if (from_g) red_min(usemin + slot, static_cast<uint32_t>(k));
-    if (on) {
-      if (record) {
-        ot[h] = tag | static_cast<uint64_t>(key) | (static_cast<uint64_t>(index) << 24);
-        ol[n_own++] = key | (static_cast<uint32_t>(index) << 24);
-      }
-#pragma unroll
-      for (int c = 0; c < C; ++c) e[c] = __dadd_rn(static_cast<double>(f[c]), -errp[c * kMaxPaletteColors + index]);
-      if (live) {
-        const int q = (t - begin) & 3;
-        acc |= static_cast<uint32_t>(index) << (8 * q);
-        if (q == 3) {
-          *reinterpret_cast<uint32_t*>(out + t - 3) = acc;
-          acc = 0;
-        } else if (t == end - 1) {
-          for (int r = 0; r <= q; ++r) out[t - q + r] = static_cast<uint8_t>(acc >> (8 * r));
+        for (int c = 0; c < 4; ++c) t4[c] = static_cast<double>(__shfl_sync(0xffffffffu, f[c], src));
+        if constexpr (kAssoc) {
+          // ClosestColor's target: beta * t with beta = QS * t.a (rd_octree.cpp:190-208).
+          const double beta = __dmul_rn(kQuantumScale, t4[3]);
+          t4[0] = __dmul_rn(beta, t4[0]);
+          t4[1] = __dmul_rn(beta, t4[1]);
+          t4[2] = __dmul_rn(beta, t4[2]);
         }
-        if (t >= end - 16) {
-          double* d = qe + 4 * (t - (end - 16));
-          const double* o = qold + 4 * (t - (end - 16));
+        const int r = tw::search_warp<kAssoc>(P, sn, t4[0], t4[1], t4[2], t4[3], lane);
+        if (lane == src) index = r;
+      }
+      if (booked) {
+        if constexpr (kAssoc) {
+          if (!present) slot = map_insert(hkeys, hmask, key, slot, im.hlist, im.hcount);
+          if (slot < 0) atomicExch(L.status, kDevBadPlan);  // key map full: cannot happen at its size
+        }
+        if (slot >= 0) red_min(gnew + slot, (static_cast<uint32_t>(k) << 8) | static_cast<uint32_t>(index));
+      }
+      if (from_g) red_min(usemin + slot, static_cast<uint32_t>(k));
+      if (on) {
+        if (record) {
+          ot[h] = tag | static_cast<uint64_t>(key) | (static_cast<uint64_t>(index) << 24);
+          ol[n_own++] = key | (static_cast<uint32_t>(index) << 24);
+        }
 #pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const double v = c < C ? e[c < C ? c : 0] : 0.0;
-            changed |= __double_as_longlong(o[c]) != __double_as_longlong(v);
-            d[c] = v;
+        for (int c = 0; c < C; ++c) e[c] = __dadd_rn(static_cast<double>(f[c]), -errp[c * kMaxPaletteColors + index]);
+        if (live) {
+          const int q = (t - begin) & 3;
+          acc |= static_cast<uint32_t>(index) << (8 * q);
+          if (q == 3) {
+            *reinterpret_cast<uint32_t*>(out + t - 3) = acc;
+            acc = 0;
+          } else if (t == end - 1) {
+            for (int r = 0; r <= q; ++r) out[t - q + r] = static_cast<uint8_t>(acc >> (8 * r));
           }
-        }
-      } else if (t >= begin - 16) {
-        double* d = qs + 4 * (t - (begin - 16));
+          if (t >= end - 16) {
+            double* d = qe + 4 * (t - (end - 16));
+            const double* o = qold + 4 * (t - (end - 16));
 #pragma unroll
-        for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
+            for (int c = 0; c < 4; ++c) {
+              const double v = c < C ? e[c < C ? c : 0] : 0.0;
+              changed |= __double_as_longlong(o[c]) != __double_as_longlong(v);
+              d[c] = v;
+            }
+          }
+        } else if (t >= begin - 16) {
+          double* d = qs + 4 * (t - (begin - 16));
+#pragma unroll
+          for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
+        }
       }
+      if constexpr (kChain) {
+        // The residual to the sum warp (every lane arrives).
+#pragma unroll
+        for (int c = 0; c < C; ++c) box->e[i & 1][c][lane] = e[c];
+        pair_arrive(&box->full_e[i & 1]);
+      }
+      return true;
+  };
+  if constexpr (kChain) {
+    // No ring here: a plain loop.  A wait that gave up ends the walk (the
+    // status word says so).
+#pragma unroll 1
+    for (int i = 0; i < warp_steps; ++i) {
+      if (!step(i & 15, i)) return;
     }
+  } else {
+    // One step per iteration, its ring slot chosen by a switch around the
+    // rotations only (sixteen unrolled steps measured 17 % slower a launch,
+    // and spill with four channels).
+#pragma unroll 1
+    for (int i = 0; i < warp_steps; ++i) step(i & 15, i);
   }
   if (active && memo) L.own_count[sid] = n_own;
   if (active) {
@@ -491,7 +634,170 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   const bool active = static_cast<int>(threadIdx.x) < ch.count && k >= front && k < stop;
   tw::Plan P;
   P.bind(smem);
-  WalkSegment<kFloat, kAssoc>(L, im, P, errp, active ? k : warp_end - 1, front, active, lane);
+  WalkSegment<kFloat, kAssoc, false>(L, im, P, errp, active ? k : warp_end - 1, front, active, lane,
+                                     nullptr);
+}
+
+// The sum warp of a pair: the 16-slot ring of running sums for one segment
+// per lane, one step ahead of the chain warp.  It hands over pixel t's sum
+// (everything but the w15 * e_{t-1} term, which the chain adds) before step t,
+// and after the residual of step i - 1 arrives it adds that residual to the
+// 15 pending pixels and refills the slot of the pixel just taken with the
+// sample 16 positions on -- the same operations in the same order as the
+// single-thread walker's rotation, so the same sums bit for bit.
+template <bool kFloat, bool kAssoc>
+__device__ __forceinline__ void WalkSums(const TswLaunch& L, const TswImage& im, int k, int front,
+                                         bool active, int lane, PairBox* box) {
+  constexpr int C = kAssoc ? 4 : 3;
+  const int sid = im.first_seg + k;
+  const int begin = k * L.seg_len;
+  const int end = active ? min(begin + L.seg_len, im.n) : begin;
+  const bool warmup = k > 0 && (L.pass == 0 ||
+                                (L.window > 0 && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
+  const int ws = (active && warmup) ? begin - min(begin, L.pass == 0 ? L.warm_len : 0) : begin;
+  const int steps = end - ws;
+  const int64_t base = im.cx_offset;
+  double R[16][C];
+  double e0[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) e0[c] = 0.0;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    double p[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) p[c] = 0.0;
+    if (ws + u < end) sample<kFloat, C>(L, base + ws + u, p);
+#pragma unroll
+    for (int c = 0; c < C; ++c) R[u][c] = p[c];
+  }
+  if (active && !warmup && k > 0) {
+    const double* q = L.q_end[(L.pass & 1) ^ 1] + static_cast<int64_t>(sid - 1) * 64;
+#pragma unroll
+    for (int m = 0; m < 15; ++m) {
+      double qm[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) qm[c] = q[4 * m + c];
+#pragma unroll
+      for (int j = 0; j <= m; ++j) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) R[j][c] = __dadd_rn(R[j][c], __dmul_rn(L.sw[m - j], qm[c]));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) e0[c] = q[60 + c];
+  }
+  const int warp_steps = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(steps));
+  if (warp_steps <= 0) return;
+  // Step 0's sum.
+#pragma unroll
+  for (int c = 0; c < C; ++c) box->s[0][c][lane] = R[0][c];
+  pair_arrive(&box->full_s[0]);
+  // Iteration i: the residual of step i - 1 (the queue's pending one for
+  // i = 0), slot i mod 16 refilled, then step i + 1's sum handed over.
+  const auto iter = [&](auto u, const int i) -> bool {
+    double p[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) p[c] = 0.0;
+    const int t = ws + i;
+    if (i < steps && t + 16 < end) sample<kFloat, C>(L, base + t + 16, p);
+    double e[C];
+    if (i == 0) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) e[c] = e0[c];
+    } else {
+      if (!pair_wait(&box->full_e[(i - 1) & 1], ((i - 1) >> 1) & 1, L.status)) return false;
+#pragma unroll
+      for (int c = 0; c < C; ++c) e[c] = box->e[(i - 1) & 1][c][lane];
+    }
+    RotateTailAt<C>(u, L.sw, R, e, p);
+    double nx[C];
+    RingAt<C>(next_slot(u), R, nx);
+#pragma unroll
+    for (int c = 0; c < C; ++c) box->s[(i + 1) & 1][c][lane] = nx[c];
+    pair_arrive(&box->full_s[(i + 1) & 1]);
+    return true;
+  };
+  const int last = warp_steps - 1;  // iterations 0 .. last - 1 hand over sums 1 .. last
+  if constexpr (kAssoc) {
+#pragma unroll 1
+    for (int i = 0; i < last; ++i) {
+      if (!iter(i & 15, i)) return;
+    }
+  } else {
+#pragma unroll 1
+    for (int i0 = 0; i0 < last; i0 += 16) {
+#define RDB_ITER(n)                                  \
+  if (i0 + (n) >= last) break;                       \
+  if (!iter(Step<(n)>{}, i0 + (n))) return;
+      RDB_ITER(0) RDB_ITER(1) RDB_ITER(2) RDB_ITER(3) RDB_ITER(4) RDB_ITER(5) RDB_ITER(6) RDB_ITER(7)
+      RDB_ITER(8) RDB_ITER(9) RDB_ITER(10) RDB_ITER(11) RDB_ITER(12) RDB_ITER(13) RDB_ITER(14) RDB_ITER(15)
+#undef RDB_ITER
+    }
+  }
+}
+
+// The paired form of the walk: 8 warps per CTA, warp w < 4 the chain warp and
+// warp w + 4 the sum warp of the same 32 segments of the chunk.  Two CTAs per
+// SM without alpha (128 registers a thread); one with alpha, whose four-channel
+// ring does not fit in 128.
+template <bool kFloat, bool kAssoc>
+__global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKernel(TswLaunch L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int chunk = blockIdx.x;
+  if (L.window > 0) {
+    chunk += front_of(L, 0, L.images[0].nsegs) / L.chunk_threads;
+    if (chunk >= L.n_chunks) return;
+  }
+  const TswChunk ch = L.chunks[chunk];
+  const TswImage& im = L.images[ch.image];
+  const int front = front_of(L, ch.image, im.nsegs);
+  const int stop = L.window > 0 ? min(front + L.window, im.nsegs) : im.nsegs;
+  if (ch.k0 + ch.count <= front || ch.k0 >= stop) return;  // nothing to walk (uniform per CTA)
+  constexpr int C = kAssoc ? 4 : 3;
+  double* errp = reinterpret_cast<double*>(smem + L.plan_smem_max);
+  // After the plan and the residual-side colours, 16-byte aligned (as the
+  // host sizes it).
+  const int box_off = (L.plan_smem_max + 4 * kMaxPaletteColors * static_cast<int>(sizeof(double)) + 15) & ~15;
+  PairBox* boxes = reinterpret_cast<PairBox*>(smem + box_off);
+  {
+    const int4* src = reinterpret_cast<const int4*>(im.plan);
+    int4* dst = reinterpret_cast<int4*>(smem);
+    for (int i = threadIdx.x; i < im.plan_smem / 16; i += blockDim.x) dst[i] = src[i];
+  }
+  if (threadIdx.x < 4 * kPairsPerCta) {
+    PairBox& b = boxes[threadIdx.x >> 2];
+    const int which = threadIdx.x & 3;
+    pair_init(which < 2 ? &b.full_s[which] : &b.full_e[which - 2]);
+  }
+  __syncthreads();
+  {
+    tw::Plan P0;
+    P0.bind(smem);
+    for (int i = threadIdx.x; i < C * kMaxPaletteColors; i += blockDim.x) {
+      const int c = i / kMaxPaletteColors, col = i - c * kMaxPaletteColors;
+      errp[i] = col < P0.h->count ? P0.rcol<kAssoc>(col)[c] : 0.0;
+    }
+  }
+  // Barrier initialisation and the staged tables, visible to every warp.
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int pair = warp % kPairsPerCta;
+  // Both warps of a pair see the same 32 segments and leave together.
+  const int warp_k0 = ch.k0 + 32 * pair;
+  const int warp_end = min(ch.k0 + ch.count, warp_k0 + 32);
+  if (warp_end <= front || warp_k0 >= ch.k0 + ch.count || warp_k0 >= stop) return;
+  const int k = warp_k0 + lane;
+  const bool active = k < warp_end && k >= front && k < stop;
+  const int kk = active ? k : warp_end - 1;
+  if (warp < kPairsPerCta) {
+    tw::Plan P;
+    P.bind(smem);
+    WalkSegment<kFloat, kAssoc, true>(L, im, P, errp, kk, front, active, lane, &boxes[pair]);
+  } else {
+    WalkSums<kFloat, kAssoc>(L, im, kk, front, active, lane, &boxes[pair]);
+  }
 }
 
 // G_new = the entries of G_prev that verified segments made; usemin cleared;
@@ -689,12 +995,31 @@ unsigned TswVerifyGrid(const TswLaunch& L, int total_segs) {
   return static_cast<unsigned>((segs + 7) / 8);
 }
 
-template <bool kFloat, bool kAssoc>
-cudaError_t LaunchWalk(const TswLaunch& L, int smem, cudaStream_t s) {
-  const cudaError_t e = AllowMaxSmem(TswWalkKernel<kFloat, kAssoc>);
-  if (e != cudaSuccess) return e;
-  TswWalkKernel<kFloat, kAssoc><<<TswWalkGrid(L), L.chunk_threads, smem, s>>>(L);
-  return cudaGetLastError();
+// The walk kernel of a launch's form and its shape: one thread per segment
+// (128-thread CTAs), or a chain warp and a sum warp per 32 segments
+// (256-thread CTAs, the same 128 segments, plus the pairs' mailboxes).
+struct WalkShape {
+  const void* fn;
+  unsigned threads;
+  std::size_t smem;
+};
+WalkShape WalkShapeOf(bool paired, bool is_float, bool assoc, int plan_smem_max) {
+  const std::size_t base = (TswSmemBytes(plan_smem_max) + 15) & ~std::size_t{15};
+  if (paired) {
+    const void* fn = assoc ? (is_float ? reinterpret_cast<const void*>(TswWalkPairKernel<true, true>)
+                                       : reinterpret_cast<const void*>(TswWalkPairKernel<false, true>))
+                           : (is_float ? reinterpret_cast<const void*>(TswWalkPairKernel<true, false>)
+                                       : reinterpret_cast<const void*>(TswWalkPairKernel<false, false>));
+    return {fn, static_cast<unsigned>(kPairCtaThreads), base + kPairsPerCta * sizeof(PairBox)};
+  }
+  const void* fn = assoc ? (is_float ? reinterpret_cast<const void*>(TswWalkKernel<true, true>)
+                                     : reinterpret_cast<const void*>(TswWalkKernel<false, true>))
+                         : (is_float ? reinterpret_cast<const void*>(TswWalkKernel<true, false>)
+                                     : reinterpret_cast<const void*>(TswWalkKernel<false, false>));
+  return {fn, 128u, base};
+}
+WalkShape WalkShapeOf(const TswLaunch& L) {
+  return WalkShapeOf(L.paired != 0, L.is_float != 0, L.assoc != 0, L.plan_smem_max);
 }
 
 }  // namespace
@@ -703,17 +1028,15 @@ std::size_t TswSmemBytes(int plan_smem_max) {
   return static_cast<std::size_t>(plan_smem_max) + 4 * kMaxPaletteColors * sizeof(double);
 }
 
-int TswResidentThreads(int plan_smem_max, int sm_count, int assoc) {
-  const int smem = static_cast<int>(TswSmemBytes(plan_smem_max));
-  const void* k = assoc ? reinterpret_cast<const void*>(TswWalkKernel<false, true>)
-                        : reinterpret_cast<const void*>(TswWalkKernel<false, false>);
-  if ((assoc ? AllowMaxSmem(TswWalkKernel<false, true>) : AllowMaxSmem(TswWalkKernel<false, false>)) !=
-      cudaSuccess) {
+int TswResidentThreads(int plan_smem_max, int sm_count, int assoc, int paired) {
+  const WalkShape w = WalkShapeOf(paired != 0, false, assoc != 0, plan_smem_max);
+  if (AllowMaxSmem(w.fn) != cudaSuccess) return 0;
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, w.fn, static_cast<int>(w.threads),
+                                                    w.smem) != cudaSuccess) {
     return 0;
   }
-  int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, 128, smem) != cudaSuccess) return 0;
-  return blocks * 128 * sm_count;
+  return blocks * 128 * sm_count;  // 128 segments per CTA in either form
 }
 
 cudaError_t LaunchTswGather(const TswLaunch& L, int64_t total, cudaStream_t s) {
@@ -730,9 +1053,11 @@ cudaError_t LaunchTswPrepare(const TswLaunch& L, cudaStream_t s) {
 
 cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s) {
   if (L.n_chunks <= 0) return cudaSuccess;
-  const int smem = static_cast<int>(TswSmemBytes(L.plan_smem_max));
-  if (L.assoc) return L.is_float ? LaunchWalk<true, true>(L, smem, s) : LaunchWalk<false, true>(L, smem, s);
-  return L.is_float ? LaunchWalk<true, false>(L, smem, s) : LaunchWalk<false, false>(L, smem, s);
+  const WalkShape w = WalkShapeOf(L);
+  cudaError_t e = AllowMaxSmem(w.fn);
+  if (e != cudaSuccess) return e;
+  void* args[] = {const_cast<TswLaunch*>(&L)};
+  return cudaLaunchKernel(w.fn, dim3(TswWalkGrid(L)), dim3(w.threads), args, w.smem, s);
 }
 
 cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) {
@@ -766,11 +1091,6 @@ cudaError_t AddKernel(cudaGraph_t g, cudaGraphNode_t* last, const void* func, di
   return e;
 }
 
-template <bool kFloat, bool kAssoc>
-const void* WalkFunc() {
-  return reinterpret_cast<const void*>(TswWalkKernel<kFloat, kAssoc>);
-}
-
 // One pass into graph g after *last: clear this parity's failures, prepare,
 // walk, check, control.
 cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int total_segs,
@@ -796,10 +1116,9 @@ cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int tota
     if (e != cudaSuccess) return e;
   }
   if (L->n_chunks > 0) {
-    const void* wf = L->assoc ? (L->is_float ? WalkFunc<true, true>() : WalkFunc<false, true>())
-                              : (L->is_float ? WalkFunc<true, false>() : WalkFunc<false, false>());
-    e = AddKernel(g, last, wf, dim3(TswWalkGrid(*L)), dim3(L->chunk_threads),
-                  static_cast<unsigned>(TswSmemBytes(L->plan_smem_max)), args1);
+    const WalkShape w = WalkShapeOf(*L);
+    e = AddKernel(g, last, w.fn, dim3(TswWalkGrid(*L)), dim3(w.threads), static_cast<unsigned>(w.smem),
+                  args1);
     if (e != cudaSuccess) return e;
   }
   if (L->use_cache && L->n_images > 0) {
@@ -828,12 +1147,7 @@ cudaError_t BuildTswLoopGraph(const TswLaunch& even, const TswLaunch& odd, int t
                               int* ctl, uint32_t* tag_dev, int max_passes, cudaGraph_t* out) {
   cudaError_t e;
   if (even.n_chunks > 0) {
-    if ((e = even.assoc ? (even.is_float ? AllowMaxSmem(TswWalkKernel<true, true>)
-                                         : AllowMaxSmem(TswWalkKernel<false, true>))
-                        : (even.is_float ? AllowMaxSmem(TswWalkKernel<true, false>)
-                                         : AllowMaxSmem(TswWalkKernel<false, false>))) != cudaSuccess) {
-      return e;
-    }
+    if ((e = AllowMaxSmem(WalkShapeOf(even).fn)) != cudaSuccess) return e;
   }
   cudaGraph_t g = nullptr;
   if ((e = cudaGraphCreate(&g, 0)) != cudaSuccess) return e;

@@ -114,6 +114,9 @@ struct TswLaunch {
   int window;
   uint8_t* walked[2];
   uint8_t* warmed;
+  // Walk form: 0 = one thread per segment; 1 = paired warps, a chain warp
+  // and a sum warp per 32 segments (same results bit for bit).
+  int paired;
   int* status;
   // Device-side loop: the own-table tag of the running pass (null: use `tag`).
   const uint32_t* tag_dev;
@@ -121,8 +124,8 @@ struct TswLaunch {
 };
 
 std::size_t TswSmemBytes(int plan_smem_max);
-// Walker threads the device holds at once (0 if the query fails).
-int TswResidentThreads(int plan_smem_max, int sm_count, int assoc);
+// Segments the device walks at once in the given form (0 if the query fails).
+int TswResidentThreads(int plan_smem_max, int sm_count, int assoc, int paired);
 // Samples of every image in visit order, into L.cx.
 cudaError_t LaunchTswGather(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
 // G_new = verified entries of G_prev, usemin cleared (memo only).

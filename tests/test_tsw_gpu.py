@@ -13,22 +13,25 @@ from stipple_b200 import synth
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("seg,warm", [(64, 16), (256, 128), (1024, 512)])
-def test_thread_segmented_matches_oracle(ctx, oracle, seg, warm):
+def test_thread_segmented_matches_oracle(ctx, oracle, seg, warm, form):
     for k, (w, h, colors) in enumerate([(256, 192, 16), (300, 211, 256), (97, 403, 64)]):
         img = synth.gradient_rgb8(w, h, 40 + k)
         t = sb.Octree(img, colors, False)
         pid = ctx.palette_from_octree(t)
         try:
-            got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=seg, warm_len=warm)
+            got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=seg, warm_len=warm,
+                                  walk_form=form)
             want, _, _ = oracle.walk_seq(synth.to_q16(img), colors, False, t.grayscale)
-            assert np.array_equal(got, want), (w, h, colors, seg, warm)
+            assert np.array_equal(got, want), (w, h, colors, seg, warm, form)
             assert ctx.last_passes >= 1
         finally:
             ctx.release_palette(pid)
 
 
-def test_thread_segmented_no_cache_and_diffusion(ctx, oracle):
+@pytest.mark.parametrize("form", [1, 2])
+def test_thread_segmented_no_cache_and_diffusion(ctx, oracle, form):
     img = synth.gradient_rgb8(400, 300, 8)
     t = sb.Octree(img, 32, False)
     pid = ctx.palette_from_octree(t)
@@ -37,14 +40,15 @@ def test_thread_segmented_no_cache_and_diffusion(ctx, oracle):
         for cache in (0, 1):
             for diff in (0.5, 1.0):
                 got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=128, warm_len=32,
-                                      use_cache=cache, diffusion=diff)
+                                      use_cache=cache, diffusion=diff, walk_form=form)
                 want, _, _ = oracle.walk_seq(q, 32, False, False, diffusion=diff, use_cache=bool(cache))
                 assert np.array_equal(got, want), (cache, diff)
     finally:
         ctx.release_palette(pid)
 
 
-def test_thread_segmented_gray_and_float(ctx, oracle):
+@pytest.mark.parametrize("form", [1, 2])
+def test_thread_segmented_gray_and_float(ctx, oracle, form):
     """A greyscale palette (the deepest tree, whose descent reads bits below the
     memo key) and RgbaF input that is not 8-bit multiples."""
     img = synth.gradient_rgb8(320, 200, 12)
@@ -53,7 +57,7 @@ def test_thread_segmented_gray_and_float(ctx, oracle):
     assert t.grayscale
     pid = ctx.palette_from_octree(t)
     try:
-        got = ctx.dither_host("seq", g, pid, seq_mode=3, seg_len=128, warm_len=64)
+        got = ctx.dither_host("seq", g, pid, seq_mode=3, seg_len=128, warm_len=64, walk_form=form)
         want, _, _ = oracle.walk_seq(synth.to_q16(g), 16, False, True)
         assert np.array_equal(got, want)
     finally:
@@ -65,7 +69,7 @@ def test_thread_segmented_gray_and_float(ctx, oracle):
     pid = ctx.palette(tree.palette, tree.child, tree.color_number, tree.number_unique, False,
                       parent=tree.parent)
     try:
-        got = ctx.dither_host("seq", q, pid, seq_mode=3, seg_len=256, warm_len=64)
+        got = ctx.dither_host("seq", q, pid, seq_mode=3, seg_len=256, warm_len=64, walk_form=form)
         want, _, _ = oracle.walk_seq(q, 64, False, False)
         assert np.array_equal(got, want)
     finally:
@@ -111,8 +115,9 @@ def test_thread_segmented_full_hd_auto(ctx, oracle):
         ctx.release_palette(pid)
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("seg,warm", [(64, 16), (256, 64)])
-def test_thread_segmented_alpha(ctx, oracle, seg, warm):
+def test_thread_segmented_alpha(ctx, oracle, seg, warm, form):
     """Alpha-associated palettes: four channels, 24-bit keys in hashed maps."""
     for k, (w, h, colors) in enumerate([(256, 192, 16), (300, 211, 256), (97, 403, 4), (640, 64, 64)]):
         img = synth.gradient_rgba8(w, h, 60 + k)
@@ -120,7 +125,7 @@ def test_thread_segmented_alpha(ctx, oracle, seg, warm):
         pid = ctx.palette_from_octree(t)
         try:
             got, rgba = ctx.dither_host("seq", img, pid, rgba=True, seq_mode=3, seg_len=seg,
-                                        warm_len=warm)
+                                        warm_len=warm, walk_form=form)
             want, out, _ = oracle.walk_seq(synth.to_q16(img), colors, True, t.grayscale)
             assert np.array_equal(got, want), (w, h, colors, seg, warm)
             assert np.array_equal(rgba.view(np.uint32), out.view(np.uint32)), (w, h, colors)
@@ -170,8 +175,9 @@ def test_thread_segmented_mixed_alpha_batch(ctx, oracle):
             ctx.release_palette(p)
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("alpha", [False, True])
-def test_host_and_device_pass_loops_agree(ctx, oracle, alpha):
+def test_host_and_device_pass_loops_agree(ctx, oracle, alpha, form):
     """The pass loop checked by the host (loop_mode=1) and the device-side loop
     in one CUDA graph (loop_mode=2) give the oracle's bytes; the device loop's
     pass limit surfaces as an error, never as an inexact result."""
@@ -181,7 +187,8 @@ def test_host_and_device_pass_loops_agree(ctx, oracle, alpha):
     try:
         want, _, _ = oracle.walk_seq(synth.to_q16(img), 64, alpha, t.grayscale)
         for mode in (1, 2, 2):  # the second device-loop call reuses the cached graph
-            got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=64, warm_len=16, loop_mode=mode)
+            got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=64, warm_len=16, loop_mode=mode,
+                                  walk_form=form)
             assert np.array_equal(got, want), mode
             assert ctx.last_passes >= 3
         with pytest.raises(sb.RdbError):
@@ -193,9 +200,10 @@ def test_host_and_device_pass_loops_agree(ctx, oracle, alpha):
         ctx.release_palette(pid)
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("alpha", [False, True])
 @pytest.mark.parametrize("window,seg", [(1, 32), (5, 32), (37, 48), (130, 64)])
-def test_thread_segmented_window(ctx, oracle, alpha, window, seg):
+def test_thread_segmented_window(ctx, oracle, alpha, window, seg, form):
     """One image walked a window of segments beyond the front each pass:
     segments entering the window start from warm-ups, the front stops at the
     window's end; both pass loops, with and without the memo table."""
@@ -208,10 +216,14 @@ def test_thread_segmented_window(ctx, oracle, alpha, window, seg):
             want, _, _ = oracle.walk_seq(q, 64, alpha, t.grayscale, use_cache=bool(cache))
             for mode in (1, 2):
                 got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=seg, warm_len=16,
-                                      seg_window=window, use_cache=cache, loop_mode=mode)
+                                      seg_window=window, use_cache=cache, loop_mode=mode,
+                                      walk_form=form)
                 assert np.array_equal(got, want), (cache, mode)
                 # The front advances at most a window per pass.
-                assert ctx.last_passes >= -(-(300 * 170) // (seg * window))
+                passes = ctx.last_passes
+                print(f"window {window} seg {seg} alpha {alpha} form {form} cache {cache} "
+                      f"mode {mode}: {passes} passes")
+                assert passes >= -(-(300 * 170) // (seg * window)), (cache, mode, passes)
     finally:
         ctx.release_palette(pid)
 
