@@ -87,6 +87,9 @@ def parse():
                     help="run only that workload's device steps (for ncu captures) and print "
                          "its timing; no JSON contract line")
     ap.add_argument("--seq-mode", type=int, default=0, help="profile cases: sequential form")
+    ap.add_argument("--walk-form", type=int, default=0,
+                    help="profile cases: segmented walk form (1 paired warps, 2 one thread a segment)")
+    ap.add_argument("--seg-len", type=int, default=0, help="profile cases: segment length (0 = tuned)")
     ap.add_argument("--size", default="3840x2160", help="profile cases: frame size WxH")
     ap.add_argument("--loop-mode", type=int, default=0,
                     help="profile cases: segmented walk pass loop (1 = host-checked, so ncu "
@@ -931,7 +934,8 @@ def profile_case(a):
         o = torch.empty((H, W), dtype=torch.uint8, device="cuda")
         jobs = [dict(pixels=d.data_ptr(), width=W, height=H, layout=lay, palette_id=pid,
                      indices=o.data_ptr())]
-        opts = {"seq_mode": a.seq_mode, "loop_mode": a.loop_mode} if a.profile_case != "jacobi" else {}
+        opts = ({"seq_mode": a.seq_mode, "loop_mode": a.loop_mode, "walk_form": a.walk_form,
+                 "seg_len": a.seg_len} if a.profile_case != "jacobi" else {})
     else:
         n = a.block_frames
         frames = [torch.from_numpy(synth.video_frame(W, H, 3, f)).cuda() for f in range(n)]

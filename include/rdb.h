@@ -390,11 +390,14 @@ typedef struct rdb_server_options {
   size_t memory_budget;   /* admission cap in bytes (0 = 90 % of free memory) */
   int workers;            /* device workers (0 = 4) */
   int max_batch;          /* requests per batch (0 = 512) */
-  int host_threads;       /* palette builders of the host form (0 = the CPUs this process may
-                             run on: its affinity mask, capped by a cgroup CPU quota) */
-  int host_palettes;      /* 0 (default): each device worker builds its batch's palettes on
-                             the device from the uploaded pixels (rdb_octree_build_device);
-                             1: host threads build them (rdb_octree_build) before admission */
+  int host_threads;       /* palette builders on the host (0 = the CPUs this process may run
+                             on: its affinity mask, capped by a cgroup CPU quota) */
+  int device_palettes;    /* 0 (default): host threads build each request's palette
+                             (rdb_octree_build) before admission, many at once; 1: each device
+                             worker builds its batch's palettes on the device from the uploaded
+                             pixels (rdb_octree_build_device), one after another -- faster per
+                             build for RGB at 256 colours, slower with alpha, and serialised on
+                             the workers, so a mixed stream is served far slower */
 } rdb_server_options;
 
 typedef struct rdb_request {
@@ -451,10 +454,10 @@ typedef struct rdb_server_stats {
 int rdb_server_create(const rdb_server_options* opts, rdb_server** out);
 /* Device bytes the server counts for `req` while it is admitted (its staging,
  * visit order, palette tables, the scratch of the engine path it takes and,
- * unless host_palettes, its palette build's scratch): a request whose bytes
+ * with device_palettes, its palette build's scratch): a request whose bytes
  * exceed the server's budget is refused at submission.  Reads the pixels
  * only to classify greyscale for a device palette build. */
-size_t rdb_request_bytes(const rdb_request* req, int host_palettes);
+size_t rdb_request_bytes(const rdb_request* req, int device_palettes);
 
 /* Non-blocking; the request (and its buffers) must outlive its completion. */
 int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket);

@@ -62,7 +62,7 @@ class Options(C.Structure):
 class ServerOptions(C.Structure):
     """rdb_server_options (include/rdb.h)."""
     _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t), ("workers", C.c_int),
-                ("max_batch", C.c_int), ("host_threads", C.c_int), ("host_palettes", C.c_int)]
+                ("max_batch", C.c_int), ("host_threads", C.c_int), ("device_palettes", C.c_int)]
 
 
 class Request(C.Structure):
@@ -671,20 +671,20 @@ class Server:
     threads, admits by device memory and batches on its device workers."""
 
     def __init__(self, device: int = 0, budget: int = 0, workers: int = 0, max_batch: int = 0,
-                 host_threads: int = 0, host_palettes: bool = False):
-        o = ServerOptions(device, budget, workers, max_batch, host_threads, int(host_palettes))
+                 host_threads: int = 0, device_palettes: bool = False):
+        o = ServerOptions(device, budget, workers, max_batch, host_threads, int(device_palettes))
         self.handle = C.c_void_p()
         _check(load().rdb_server_create(C.byref(o), C.byref(self.handle)))
         self._live: dict[int, tuple] = {}
 
     @staticmethod
     def request_bytes(img: np.ndarray, colors: int, engine: str | int = "seq",
-                      alpha: bool = False, rgba: bool = False, host_palettes: bool = False,
+                      alpha: bool = False, rgba: bool = False, device_palettes: bool = False,
                       **opts) -> int:
         """Device bytes a server counts for this request while admitted
         (rdb_request_bytes)."""
         img, r, _, _ = Server._request(img, colors, engine, alpha, rgba, opts)
-        return int(load().rdb_request_bytes(C.byref(r), int(host_palettes)))
+        return int(load().rdb_request_bytes(C.byref(r), int(device_palettes)))
 
     @staticmethod
     def _request(img, colors, engine, alpha, rgba, opts):

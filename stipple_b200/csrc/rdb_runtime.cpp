@@ -26,6 +26,7 @@ thread_local std::string g_error;
 constexpr std::size_t kMaxOrders = 1024;  // resident geometries before eviction
 constexpr std::size_t kOrderCacheBytes = std::size_t{1} << 30;  // and their bytes
 constexpr int kMaxAlphaSlabs = 64;  // plain walk: alpha memo slabs (32 MiB each) per launch
+constexpr int kBatchWindowMin = 256;  // segmented walk of several images: the least window each
 
 std::size_t RowStride(const rdb_job& j) {
   return j.row_stride ? j.row_stride : static_cast<std::size_t>(j.width) * BytesPerPixel(j.layout);
@@ -1634,11 +1635,13 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   bool paired = o.walk_form == 1 || (o.walk_form == 0 && n == 1);
   if (paired && TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0, 1) <= 0) paired = false;
   const int64_t resident = std::max(1, TswResidentThreads(plan_max, sm_count_, assoc ? 1 : 0, paired ? 1 : 0));
-  // One image walks a window of resident segments beyond its front each pass
-  // (rdb_tsw.h): segments can then be shorter than "all of them resident"
-  // allows -- a pass costs seg_len steps, and the front advances about as far
-  // per pass in positions, so shorter segments cost fewer steps in total.
-  const bool windowed = n == 1 && o.seg_window >= 0;
+  // Each image walks a window of segments beyond its front each pass
+  // (rdb_tsw.h) -- one image the resident segments, several a share of them
+  // each -- so segments can be shorter than "all of them resident" allows: a
+  // pass costs seg_len steps, and the front advances about as far per pass in
+  // positions, so shorter segments cost fewer steps in total, and no pass
+  // walks segments far past a front only to walk them again.
+  const bool windowed = o.seg_window >= 0;
   if (seg_len <= 0) {
     const int rule = static_cast<int>(std::min<int64_t>(16384, (all_px + resident - 1) / resident));
     int bucket = 0;
@@ -1736,7 +1739,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   }
   if (int rc = Reserve(&tsw_images_, imgs.size() * sizeof(TswImage), "segmented walk images")) return rc;
   if (int rc = Reserve(&tsw_chunks_, chunks.size() * sizeof(TswChunk), "segment chunks")) return rc;
-  if (int rc = Reserve(&tsw_bad_, 2 * static_cast<std::size_t>(n) * sizeof(int), "verification flags")) return rc;
+  if (int rc = Reserve(&tsw_bad_, 3 * static_cast<std::size_t>(n) * sizeof(int), "verification flags")) return rc;
   if (int rc = Reserve(&tsw_q_, 3 * q_bytes, "segment queues")) return rc;
   if (int rc = Reserve(&tsw_cx_, static_cast<std::size_t>(positions) * (is_float ? 16 : 4), "gathered samples")) return rc;
   if (int rc = Reserve(&tsw_chosen_, static_cast<std::size_t>(positions), "segment indices")) return rc;
@@ -1800,11 +1803,25 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.warmed = L.changed + 3 * static_cast<std::size_t>(total);
   L.paired = paired ? 1 : 0;
   L.window = 0;
+  L.win = nullptr;
   if (windowed) {
     const int w = o.seg_window > 0 ? o.seg_window : static_cast<int>(std::min<int64_t>(resident, total));
-    if (w < total) L.window = std::max(1, w);
+    if (w < total) {
+      if (n == 1) {
+        L.window = std::max(1, w);
+      } else {
+        L.win = bad + 2 * n;
+        L.resident_segs = std::max(1, w);
+        L.win_min = kBatchWindowMin;
+      }
+    }
   }
-  if (L.window > 0) cudaMemsetAsync(L.walked[0], 0, 2 * static_cast<std::size_t>(total), s);
+  if (L.window > 0 || L.win) cudaMemsetAsync(L.walked[0], 0, 2 * static_cast<std::size_t>(total), s);
+  L.walk_count = nullptr;
+  if (profiling_) {
+    L.walk_count = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(status_.ptr) + 64);
+    cudaMemsetAsync(L.walk_count, 0, sizeof(unsigned long long), s);
+  }
   L.status = static_cast<int*>(status_.ptr);
   scaled_weights(o.diffusion, L.sw);
 
@@ -1826,6 +1843,12 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
     }
   }
   if ((e = LaunchTswGather(L, positions, s)) != cudaSuccess) return CudaFail(e, "sample gather");
+  if (L.win) {
+    // Pass 0's windows, from every front at 0 (bad[1] as pass 0 reads it).
+    TswLaunch first = L;
+    first.pass = 1;
+    if ((e = LaunchTswWindows(first, s)) != cudaSuccess) return CudaFail(e, "segment windows");
+  }
 
   const int max_passes_opt = o.max_passes > 0 ? o.max_passes : 1 << 30;
   const bool device_loop = o.loop_mode == 2 || (o.loop_mode == 0 && !profiling_);
@@ -1885,6 +1908,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       if ((e = LaunchTswPrepare(L, s)) != cudaSuccess) return CudaFail(e, "first-touch map");
       if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return CudaFail(e, "segmented walk");
       if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return CudaFail(e, "verification");
+      if ((e = LaunchTswWindows(L, s)) != cudaSuccess) return CudaFail(e, "segment windows");
     }
     if ((e = cudaGraphLaunch(loop_exec_, s)) != cudaSuccess) return CudaFail(e, "pass-loop graph launch");
     if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
@@ -1933,6 +1957,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       if ((e = LaunchTswWalk(L, s)) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "segmented walk"));
       if (profiling_) cudaEventRecord(walk_ev_[2 * k + 1], s);
       if ((e = LaunchTswVerify(L, total, s)) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "verification"));
+      if ((e = LaunchTswWindows(L, s)) != cudaSuccess) return drain(RDB_E_CUDA, CudaErr(e, "segment windows"));
       int* slot = ring_h_ + static_cast<std::size_t>(k) * slot_ints;
       if ((e = cudaMemcpyAsync(slot, cur, static_cast<std::size_t>(n) * sizeof(int),
                                cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
@@ -1941,7 +1966,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
         return drain(RDB_E_CUDA, CudaErr(e, "verification readback"));
       }
       // walk, checks, [prepare, keys, alpha-key classification]
-      if (profiling_) stats_.launches += 1 + 1 + (use_cache ? (assoc ? 3 : 2) : 0);
+      if (profiling_) stats_.launches += 1 + 1 + (use_cache ? (assoc ? 3 : 2) : 0) + (L.win ? 1 : 0);
       ++issued;
     }
     if (checked == issued) return drain(RDB_E_DEVICE, "segmented walk did not converge within the pass limit");
@@ -1957,20 +1982,6 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       stats_.walk_ms += ms;
       stats_.walk_launches += 1;
       stats_.passes += 1;
-      for (int i = 0; i < n; ++i) {
-        const TswImage& im = imgs[static_cast<std::size_t>(i)];
-        const int f0 = std::max(front[static_cast<std::size_t>(i)], 0);
-        if (f0 >= im.nsegs) continue;
-        // Walked this pass: segments [f0, stop), plus the warm-ups of pass 0.
-        const int stop = L.window > 0 ? std::min(im.nsegs, f0 + L.window) : im.nsegs;
-        stats_.walk_positions += std::min<int64_t>(im.n, static_cast<int64_t>(stop) * seg_len) -
-                                 static_cast<int64_t>(f0) * seg_len;
-        if (checked == 0) {
-          for (int kk = std::max(f0, 1); kk < stop; ++kk) {
-            stats_.walk_positions += std::min(kk * seg_len, warm_len);
-          }
-        }
-      }
     }
     // The verified prefix of every unfinished image grows by at least one
     // segment a pass (its first walked segment started from exact state);
@@ -2002,9 +2013,14 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   loop_pending_ = false;  // this call's count, not an earlier device loop's
   if ((e = LaunchTswScatter(L, positions, s)) != cudaSuccess) return CudaFail(e, "index scatter");
   if (profiling_) {
-    stats_.launches += 2;  // gather, scatter
+    stats_.launches += 2 + (L.win ? 1 : 0);  // gather, scatter, first windows
     stats_.seg_len = seg_len;
     stats_.chains = total;
+    unsigned long long walked = 0;
+    if (cudaMemcpyAsync(&walked, L.walk_count, sizeof(walked), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess) {
+      stats_.walk_positions += static_cast<int64_t>(walked);
+    }
   }
   return RDB_OK;
 }

@@ -3,10 +3,10 @@
 // Stages joined by queues under one mutex:
 //   build    the request's colour tree (the reference's ColorTree::Build
 //            semantics, greyscale rule of src/rd_cli.cpp:2452-2456).  By
-//            default the device worker builds it from the uploaded pixels
-//            (rdb_octree_build_device) at the start of the batch call; with
-//            host_palettes, host threads build it (rdb_octree_build) before
-//            admission, parallel by request;
+//            default host threads build it (rdb_octree_build) before
+//            admission, parallel by request; with device_palettes the device
+//            worker builds it from the uploaded pixels
+//            (rdb_octree_build_device) at the start of the batch call;
 //   admit    a request waits until the device-memory estimate of all
 //            admitted requests plus its own fits the budget (first fit in
 //            arrival order, so one large request does not block small ones
@@ -288,7 +288,7 @@ void rdb_server::Work(int index) {
     std::vector<rdb_host_job> jobs(batch.size());
     std::vector<int> colors(batch.size()), assoc(batch.size());
     std::vector<double> build_ms(batch.size(), 0.0);
-    const bool on_device = o.host_palettes == 0;
+    const bool on_device = o.device_palettes != 0;
     int rc = crc;
     for (std::size_t i = 0; i < batch.size() && rc == RDB_OK; ++i) {
       if (!on_device) rc = rdb_palette_from_octree(ctx, batch[i]->tree, &pids[i]);
@@ -390,7 +390,7 @@ int rdb_server_create(const rdb_server_options* opts, rdb_server** out) {
     return rdb::Fail(RDB_E_CUDA, "rdb_server_create: cudaMemGetInfo failed");
   }
   s->budget = s->o.memory_budget ? std::min(s->o.memory_budget, (free_b / 10) * 9) : (free_b / 10) * 9;
-  if (s->o.host_palettes) {
+  if (!s->o.device_palettes) {
     for (int i = 0; i < s->o.host_threads; ++i) s->builders.emplace_back([s] { s->Build(); });
   }
   s->ctxs.assign(static_cast<std::size_t>(s->o.workers), nullptr);
@@ -401,9 +401,9 @@ int rdb_server_create(const rdb_server_options* opts, rdb_server** out) {
   return RDB_OK;
 }
 
-size_t rdb_request_bytes(const rdb_request* req, int host_palettes) {
+size_t rdb_request_bytes(const rdb_request* req, int device_palettes) {
   if (!req || !req->pixels || req->width < 1 || req->height < 1) return 0;
-  return EstimateBytes(*req, host_palettes == 0);
+  return EstimateBytes(*req, device_palettes != 0);
 }
 
 int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
@@ -416,7 +416,7 @@ int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
   }
   Req* q = new Req();
   q->r = *req;
-  q->bytes = EstimateBytes(*req, s->o.host_palettes == 0);
+  q->bytes = EstimateBytes(*req, s->o.device_palettes != 0);
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) {
     delete q;
@@ -435,7 +435,7 @@ int rdb_server_submit(rdb_server* s, const rdb_request* req, uint64_t* ticket) {
   s->all[q->ticket] = q;
   ++s->pending;
   *ticket = q->ticket;
-  if (s->o.host_palettes) {
+  if (!s->o.device_palettes) {
     s->incoming.push_back(q);
     s->cv_build.notify_one();
   } else {

@@ -29,6 +29,12 @@ __device__ __forceinline__ int front_of(const TswLaunch& L, int image, int nsegs
   return b < nsegs ? b : nsegs;
 }
 
+// Segments image `image` walks beyond its front this pass (0 = all).
+__device__ __forceinline__ int window_of(const TswLaunch& L, int image) {
+  return L.win ? L.win[image] : L.window;
+}
+__device__ __forceinline__ bool windowed(const TswLaunch& L) { return L.window > 0 || L.win != nullptr; }
+
 __device__ __forceinline__ int find_image(const TswImage* imgs, int n, int64_t pos) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
@@ -326,7 +332,7 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   // warm-up -- it lies far past the front, and a warm-up would hold up the
   // whole launch while buying almost no progress.
   const bool warmup = k > 0 && (L.pass == 0 ||
-                                (L.window > 0 && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
+                                (windowed(L) && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
   const int ws = (active && warmup) ? begin - min(begin, L.pass == 0 ? L.warm_len : 0) : begin;
   if (active && warmup && ws == begin) {
     // No warm-up position writes the start queue: it is the empty one.
@@ -579,10 +585,15 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
 #pragma unroll 1
     for (int i = 0; i < warp_steps; ++i) step(i & 15, i);
   }
+  if (L.walk_count) {
+    const unsigned mine = active ? static_cast<unsigned>(steps) : 0u;
+    const unsigned warp_total = __reduce_add_sync(0xffffffffu, mine);
+    if (lane == 0) atomicAdd(L.walk_count, static_cast<unsigned long long>(warp_total));
+  }
   if (active && memo) L.own_count[sid] = n_own;
   if (active) {
     L.changed[sid] = changed ? 1 : 0;
-    if (L.window > 0) {
+    if (windowed(L)) {
       L.walked[L.pass & 1][sid] = 1;
       L.warmed[sid] = warmup ? 1 : 0;
     }
@@ -602,7 +613,8 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   const TswChunk ch = L.chunks[chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
-  const int stop = L.window > 0 ? min(front + L.window, im.nsegs) : im.nsegs;
+  const int wnd = window_of(L, ch.image);
+  const int stop = wnd > 0 ? min(front + wnd, im.nsegs) : im.nsegs;
   if (ch.k0 + ch.count <= front || ch.k0 >= stop) return;  // nothing to walk (uniform per CTA)
   {
     const int4* src = reinterpret_cast<const int4*>(im.plan);
@@ -653,7 +665,7 @@ __device__ __forceinline__ void WalkSums(const TswLaunch& L, const TswImage& im,
   const int begin = k * L.seg_len;
   const int end = active ? min(begin + L.seg_len, im.n) : begin;
   const bool warmup = k > 0 && (L.pass == 0 ||
-                                (L.window > 0 && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
+                                (windowed(L) && k > front && !L.walked[(L.pass & 1) ^ 1][sid - 1]));
   const int ws = (active && warmup) ? begin - min(begin, L.pass == 0 ? L.warm_len : 0) : begin;
   const int steps = end - ws;
   const int64_t base = im.cx_offset;
@@ -751,7 +763,8 @@ __global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKe
   const TswChunk ch = L.chunks[chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
-  const int stop = L.window > 0 ? min(front + L.window, im.nsegs) : im.nsegs;
+  const int wnd = window_of(L, ch.image);
+  const int stop = wnd > 0 ? min(front + wnd, im.nsegs) : im.nsegs;
   if (ch.k0 + ch.count <= front || ch.k0 >= stop) return;  // nothing to walk (uniform per CTA)
   constexpr int C = kAssoc ? 4 : 3;
   double* errp = reinterpret_cast<double*>(smem + L.plan_smem_max);
@@ -875,9 +888,10 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
   if (k >= im.nsegs) return;
   const int front = front_of(L, lo, im.nsegs);
   if (k < front) return;  // verified earlier, not walked
-  if (L.window > 0 && k >= front + L.window) {
+  const int wnd = window_of(L, lo);
+  if (wnd > 0 && k >= front + wnd) {
     // Not walked this pass: the front stops at the window's end.
-    if (k == front + L.window && lane == 0) atomicMin(L.bad[L.pass & 1] + lo, k);
+    if (k == front + wnd && lane == 0) atomicMin(L.bad[L.pass & 1] + lo, k);
     return;
   }
   // Only the image's FIRST failure matters: segments past one already found
@@ -890,7 +904,7 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
     // which the predecessor compared with its new one (L.changed), or from a
     // warm-up (pass 0, and segments entering a window), whose queue is
     // compared with the predecessor's end queue itself.
-    if (L.pass == 0 || (L.window > 0 && L.warmed[sid])) {
+    if (L.pass == 0 || (windowed(L) && L.warmed[sid])) {
       const double* a = L.q_start + static_cast<int64_t>(sid) * 64;
       const double* b = L.q_end[L.pass & 1] + static_cast<int64_t>(sid - 1) * 64;
       for (int i = lane; i < 64; i += 32) {
@@ -937,6 +951,31 @@ __global__ void TswScatter(TswLaunch L, int64_t total) {
     const float4 pc = reinterpret_cast<const float4*>(im.plan + h->off_out)[index];
     const float a = h->assoc ? pc.w : load_sample(im.pixels, im.layout, im.row_stride, im.width, pix).w;
     im.rgba_out[pix] = make_float4(pc.x, pc.y, pc.z, a);
+  }
+}
+
+// Per-image windows for the next pass (one block): every unfinished image
+// gets its share of the resident segments in proportion to the segments it
+// has left, at least win_min and at most what it has left.
+__global__ void TswWindows(TswLaunch L) {
+  __shared__ long long total;
+  if (threadIdx.x == 0) total = 0;
+  __syncthreads();
+  const int* bad = L.bad[L.pass & 1];
+  long long mine = 0;
+  for (int i = threadIdx.x; i < L.n_images; i += blockDim.x) {
+    const int ns = L.images[i].nsegs;
+    mine += ns - min(bad[i], ns);
+  }
+  atomicAdd(reinterpret_cast<unsigned long long*>(&total), static_cast<unsigned long long>(mine));
+  __syncthreads();
+  const long long all = total > 0 ? total : 1;
+  for (int i = threadIdx.x; i < L.n_images; i += blockDim.x) {
+    const int ns = L.images[i].nsegs;
+    const long long rem = ns - min(bad[i], ns);
+    long long w = (static_cast<long long>(L.resident_segs) * rem + all - 1) / all;
+    w = max(w, static_cast<long long>(L.win_min));
+    L.win[i] = static_cast<int>(max(1ll, min(w, rem)));
   }
 }
 
@@ -1060,6 +1099,12 @@ cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s) {
   return cudaLaunchKernel(w.fn, dim3(TswWalkGrid(L)), dim3(w.threads), args, w.smem, s);
 }
 
+cudaError_t LaunchTswWindows(const TswLaunch& L, cudaStream_t s) {
+  if (!L.win || L.n_images <= 0) return cudaSuccess;
+  TswWindows<<<1, 256, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
 cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) {
   if (L.use_cache && L.n_images > 0) {
     TswVerifyKeys<<<dim3(kKeys / 256, L.n_images), 256, 0, s>>>(L);
@@ -1135,6 +1180,10 @@ cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int tota
     void* args2[] = {L, &total_segs};
     e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifySegments), dim3(TswVerifyGrid(*L, total_segs)),
                   dim3(256), 0, args2);
+    if (e != cudaSuccess) return e;
+  }
+  if (L->win && L->n_images > 0) {
+    e = AddKernel(g, last, reinterpret_cast<const void*>(TswWindows), dim3(1), dim3(256), 0, args1);
     if (e != cudaSuccess) return e;
   }
   void* args3[] = {L, h, ctl, tag_dev, max_passes};

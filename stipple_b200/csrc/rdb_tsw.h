@@ -112,12 +112,23 @@ struct TswLaunch {
   // cache-free warm-up, as in pass 0 (walked[pass & 1] marks the walked ones,
   // warmed[] the ones that started from a warm-up this pass).
   int window;
+  // Per-image windows (launches of several images; null = none): image i
+  // walks segments [front, front + win[i]) each pass.  TswWindows sets them
+  // after every pass from the segments each image has left: resident_segs
+  // shared in proportion, at least win_min each, so the largest image, whose
+  // passes are the launch's critical path, gets the widest window.
+  int* win;
+  int resident_segs;
+  int win_min;
   uint8_t* walked[2];
   uint8_t* warmed;
   // Walk form: 0 = one thread per segment; 1 = paired warps, a chain warp
   // and a sum warp per 32 segments (same results bit for bit).
   int paired;
   int* status;
+  // Profiling (null otherwise): positions walked, warm-ups included, summed
+  // over the launches.
+  unsigned long long* walk_count;
   // Device-side loop: the own-table tag of the running pass (null: use `tag`).
   const uint32_t* tag_dev;
   double sw[16];
@@ -133,6 +144,9 @@ cudaError_t LaunchTswPrepare(const TswLaunch& L, cudaStream_t s);
 cudaError_t LaunchTswWalk(const TswLaunch& L, cudaStream_t s);
 // The three checks; the first failing segment per image into L.bad[pass & 1].
 cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s);
+// Per-image windows for the next pass from the fronts in L.bad[L.pass & 1]
+// (no-op without L.win).
+cudaError_t LaunchTswWindows(const TswLaunch& L, cudaStream_t s);
 // Indices (and RgbaF output) of every position into the images.
 cudaError_t LaunchTswScatter(const TswLaunch& L, int64_t total_positions, cudaStream_t s);
 

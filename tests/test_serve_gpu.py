@@ -2,8 +2,8 @@
 and engines submitted concurrently gives every request the same bytes as the
 same request alone (its palette built by the host builder); admission keeps
 within a tight budget; requests larger than the budget are refused at
-submission.  Both palette paths: built on the device by the worker (the
-default) and by host threads (host_palettes)."""
+submission.  Both palette paths: built by host threads (the default) and by
+the device workers (device_palettes)."""
 from __future__ import annotations
 
 import threading
@@ -40,10 +40,10 @@ def _alone(ctx, img, colors, engine, alpha):
         ctx.release_palette(pid)
 
 
-@pytest.mark.parametrize("host_palettes", [False, True])
-def test_mixed_stream_equals_each_request_alone(ctx, host_palettes):
+@pytest.mark.parametrize("device_palettes", [False, True])
+def test_mixed_stream_equals_each_request_alone(ctx, device_palettes):
     reqs = _mix(48, 3)
-    srv = sb.Server(workers=3, max_batch=16, host_palettes=host_palettes)
+    srv = sb.Server(workers=3, max_batch=16, device_palettes=device_palettes)
     try:
         tickets = [None] * len(reqs)
 
@@ -72,16 +72,16 @@ def test_mixed_stream_equals_each_request_alone(ctx, host_palettes):
         assert info["status"] == 0 and info["total_ms"] >= info["device_ms"]
 
 
-@pytest.mark.parametrize("host_palettes", [False, True])
-def test_admission_budget(ctx, host_palettes):
+@pytest.mark.parametrize("device_palettes", [False, True])
+def test_admission_budget(ctx, device_palettes):
     reqs = _mix(12, 7)
     # Room for about two of the largest requests at once (rdb_request_bytes:
     # the bound the server admits by), so requests wait for each other and
     # idle workers release their cached buffers to let the next one in.
-    need = [sb.Server.request_bytes(img, c, e, alpha=a, host_palettes=host_palettes)
+    need = [sb.Server.request_bytes(img, c, e, alpha=a, device_palettes=device_palettes)
             for img, c, e, a in reqs]
     budget = 2 * max(need) + (1 << 20)
-    srv = sb.Server(workers=2, budget=budget, host_palettes=host_palettes)
+    srv = sb.Server(workers=2, budget=budget, device_palettes=device_palettes)
     try:
         tickets = [srv.submit(img, c, e, alpha=a) for img, c, e, a in reqs]
         outs = [srv.wait(t)[0] for t in tickets]
@@ -90,7 +90,7 @@ def test_admission_budget(ctx, host_palettes):
         assert st["peak_admitted_bytes"] <= budget
         assert st["completed"] == len(reqs) and st["failed"] == 0
         big = synth.gradient_rgb8(2048, 2048, 1)
-        assert sb.Server.request_bytes(big, 16, "seq", host_palettes=host_palettes) > budget
+        assert sb.Server.request_bytes(big, 16, "seq", device_palettes=device_palettes) > budget
         with pytest.raises(sb.RdbError):
             srv.submit(big, 16, "seq")
     finally:

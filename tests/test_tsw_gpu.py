@@ -240,3 +240,29 @@ def test_thread_segmented_window_float(ctx, oracle):
         assert np.array_equal(got, want)
     finally:
         ctx.release_palette(pid)
+
+
+@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("window", [3, 40, 0, -1])
+def test_thread_segmented_batch_windows(ctx, oracle, window, form):
+    """Several images in one call, each walking its own window of segments
+    past its front, the windows re-shared after every pass by the segments
+    each image has left (window: the resident total shared out, 0 = the
+    device's resident segments, -1 = no windows); both pass loops."""
+    sizes = [(300, 170), (64, 140), (511, 97), (128, 128), (97, 61)]
+    imgs, pids, want = [], [], []
+    for k, (w, h) in enumerate(sizes):
+        img = synth.gradient_rgb8(w, h, 120 + k)
+        t = sb.Octree(img, [64, 16, 256, 8, 32][k], False)
+        pids.append(ctx.palette_from_octree(t))
+        imgs.append(img)
+        want.append(oracle.walk_seq(synth.to_q16(img), [64, 16, 256, 8, 32][k], False, t.grayscale)[0])
+    try:
+        for mode in (1, 2):
+            got = ctx.dither_host("seq", imgs, pids, seq_mode=3, seg_len=32, warm_len=16,
+                                  seg_window=window, loop_mode=mode, walk_form=form)
+            for k in range(len(imgs)):
+                assert np.array_equal(got[k], want[k]), (sizes[k], mode)
+    finally:
+        for p in pids:
+            ctx.release_palette(p)
