@@ -272,16 +272,19 @@ typedef struct rdb_options {
                            with its memo table off); 1 = the point iteration with the
                            truncated inverse filter (jacobi_taps, jacobi_fp64), as the
                            reference's approx engine */
-  int seg_window;       /* segmented thread walk of ONE image: segments walked per pass beyond
-                           the verified front (0 = automatic: as many as the device holds
-                           resident at once; -1 = every unverified segment each pass) */
+  int seg_window;       /* segmented thread walk: segments walked per pass beyond the verified
+                           front.  One image: 0 = automatic, as many as the device holds
+                           resident at once.  Several: > 0 shares that many among the images
+                           after every pass, in proportion to the segments each has left (at
+                           least 256 each); 0 = none.  -1 = every unverified segment each pass. */
   int walk_form;        /* segmented thread walk: 1 = paired warps: per 32 segments a chain warp
                            runs each step's dependent chain and a sum warp keeps the running
                            sums of the pending pixels, handing each over through shared memory
                            (a shorter step, fewer segments resident); 2 = one thread per
                            segment doing both (more segments resident); 0 = automatic: paired
-                           for one image, whose walk is latency-bound, one thread per segment
-                           for several, whose walk is throughput-bound.  Same results. */
+                           for one image without alpha, whose walk is latency-bound, one
+                           thread per segment for several (throughput-bound) and for alpha
+                           palettes (whose paired form fits one CTA per SM).  Same results. */
 } rdb_options;
 
 void rdb_options_default(rdb_options* o);

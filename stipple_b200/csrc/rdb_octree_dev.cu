@@ -133,57 +133,83 @@ __device__ __forceinline__ int find_key(const uint64_t* keys, int n, uint64_t k)
   return -1;
 }
 
-// One thread per node: its error from the first loop's value, then every
+// One warp per node: its error from the first loop's value, then every
 // contribution in run order; and the sum of its running values (what the root
-// gains from it).
+// gains from it).  The 32 lanes load 32 contributions at a time and the warp
+// adds them one by one in order (every lane keeps the same two chains), so
+// the sums are the sequential ones bit for bit while the loads run in
+// parallel -- a node can hold millions of contributions.
 __global__ void NodeSums(const OctreeRowsLaunch L, const uint64_t* ukeys, const int* offset,
                          const int* count, const int* nseg, const double* vals, double* qerr,
                          double* gain) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (s >= *nseg) return;
   const int at = find_key(L.init_keys, L.init_n, ukeys[s]);
   double acc = at >= 0 ? L.init_qerr[at] : 0.0;
   double g = 0.0;
   const double* v = vals + offset[s];
   const int n = count[s];
-  for (int i = 0; i < n; ++i) {
-    acc = __dadd_rn(acc, v[i]);
-    g = __dadd_rn(g, acc);
+  for (int base = 0; base < n; base += 32) {
+    const double mine = base + lane < n ? v[base + lane] : 0.0;
+    const int m = min(32, n - base);
+    for (int j = 0; j < m; ++j) {
+      acc = __dadd_rn(acc, __shfl_sync(0xffffffffu, mine, j));
+      g = __dadd_rn(g, acc);
+    }
   }
-  qerr[s] = acc;
-  gain[s] = g;
+  if (lane == 0) {
+    qerr[s] = acc;
+    gain[s] = g;
+  }
 }
 
-// One thread per leaf: count and totals, runs in order (rd_octree.cpp:355-359).
+// One warp per leaf: count and totals, runs in order (rd_octree.cpp:355-359).
+// Each lane forms one run's four weighted terms; the warp adds them in run
+// order, 32 runs at a time.
 __global__ void LeafSums(const OctreeRowsLaunch L, const uint64_t* ukeys, const int* offset,
                          const int* count, const int* nseg, const int* runs_sorted,
                          const int* first, int runs, uint64_t* number, double* totals) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (s >= *nseg) return;
   const int at = find_key(L.init_keys, L.init_n, ukeys[s]);
-  uint64_t num = at >= 0 ? L.init_count[at] : 0;
+  unsigned long long num = at >= 0 ? L.init_count[at] : 0;
   double t[4] = {0.0, 0.0, 0.0, 0.0};
   if (at >= 0) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) t[c] = L.init_total[4 * at + c];
   }
-  for (int i = 0; i < count[s]; ++i) {
-    const int r = runs_sorted[offset[s] + i];
-    const int64_t p = first[r];
-    const int64_t next = r + 1 < runs ? first[r + 1] : L.pixels_n;
-    const double weight = static_cast<double>(next - p);
-    double px[4];
-    associate(L.assoc != 0, pixel_at(L, p), px);
-    const double w = __dmul_rn(weight, kQuantumScale);
-    num += static_cast<uint64_t>(next - p);
-    t[0] = __dadd_rn(t[0], __dmul_rn(w, static_cast<double>(clamp_pixel(px[0]))));
-    t[1] = __dadd_rn(t[1], __dmul_rn(w, static_cast<double>(clamp_pixel(px[1]))));
-    t[2] = __dadd_rn(t[2], __dmul_rn(w, static_cast<double>(clamp_pixel(px[2]))));
-    t[3] = __dadd_rn(t[3], __dmul_rn(w, static_cast<double>(clamp_pixel(L.assoc ? px[3] : kOpaqueAlpha))));
-  }
-  number[s] = num;
+  const int n = count[s];
+  for (int base = 0; base < n; base += 32) {
+    double term[4] = {0.0, 0.0, 0.0, 0.0};
+    unsigned long long run_len = 0;
+    if (base + lane < n) {
+      const int r = runs_sorted[offset[s] + base + lane];
+      const int64_t p = first[r];
+      const int64_t next = r + 1 < runs ? first[r + 1] : L.pixels_n;
+      double px[4];
+      associate(L.assoc != 0, pixel_at(L, p), px);
+      const double w = __dmul_rn(static_cast<double>(next - p), kQuantumScale);
+      run_len = static_cast<unsigned long long>(next - p);
+      term[0] = __dmul_rn(w, static_cast<double>(clamp_pixel(px[0])));
+      term[1] = __dmul_rn(w, static_cast<double>(clamp_pixel(px[1])));
+      term[2] = __dmul_rn(w, static_cast<double>(clamp_pixel(px[2])));
+      term[3] = __dmul_rn(w, static_cast<double>(clamp_pixel(L.assoc ? px[3] : kOpaqueAlpha)));
+    }
+    // A run lies within one row, so 32 of them sum below 2^32.
+    num += __reduce_add_sync(0xffffffffu, static_cast<unsigned>(run_len));
+    const int m = min(32, n - base);
+    for (int j = 0; j < m; ++j) {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) totals[4 * s + c] = t[c];
+      for (int c = 0; c < 4; ++c) t[c] = __dadd_rn(t[c], __shfl_sync(0xffffffffu, term[c], j));
+    }
+  }
+  if (lane == 0) {
+    number[s] = num;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) totals[4 * s + c] = t[c];
+  }
 }
 
 unsigned Blocks(int64_t n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
@@ -332,8 +358,9 @@ cudaError_t ClassifyRowsDevice(const OctreeRowsLaunch& L, void* scratch, std::si
   if ((e = cub::DeviceScan::ExclusiveSum(temp, need, ucount, uoff, n[0], s)) != cudaSuccess) return e;
   need = temp_bytes;
   if ((e = cub::DeviceScan::ExclusiveSum(temp, need, lcount, loff, n[1], s)) != cudaSuccess) return e;
-  NodeSums<<<Blocks(n[0], 64), 64, 0, s>>>(L, ukeys, uoff, ucount, nseg, dv.Current(), qerr, gain);
-  LeafSums<<<Blocks(n[1], 64), 64, 0, s>>>(L, lukeys, loff, lcount, nseg + 1, lr.Current(), first, runs,
+  // One warp per node / leaf, eight per block.
+  NodeSums<<<Blocks(n[0], 8), 256, 0, s>>>(L, ukeys, uoff, ucount, nseg, dv.Current(), qerr, gain);
+  LeafSums<<<Blocks(n[1], 8), 256, 0, s>>>(L, lukeys, loff, lcount, nseg + 1, lr.Current(), first, runs,
                                            lnum, ltot);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   out->keys.resize(static_cast<std::size_t>(n[0]));
