@@ -36,9 +36,10 @@ sys.path.insert(0, ROOT)
 HEADLINE = dict(width=3840, height=2160, colors=256, seed=1)
 # Algorithmic bytes per pixel of the path: 3 B RGB8 sample in, 1 B index out.
 ALG_BYTES_PER_PX = 4
-# DRAM bytes (read + write) of one TswWalkKernel launch of the 4K walk, from
-# one ncu capture (profiles/tsw_walk_4k_rgb8_256c.md).
-TSW_TRAFFIC_PER_LAUNCH = 64074496 + 4203008
+# DRAM bytes (read + write) of one walk launch of the 4K walk in its default
+# form (TswWalkPairKernel: 96-position segments, a window of the resident
+# ones), from one ncu capture (profiles/tsw_walk_pair_4k_rgb8_256c.md).
+TSW_TRAFFIC_PER_LAUNCH = 37430016 + 622080
 # The per-step dependent path of the thread walker, as a sum of measured
 # latencies (rdb_probe_latency on the same GPU): the head's DMUL and DADD,
 # double -> float (clamp), float -> int and the byte rule's integer ops, the
@@ -410,7 +411,7 @@ def run_ours(a, rank: int, world: int):
            "h2d_bytes_per_step": int(img.nbytes), "d2h_bytes_per_step": int(W * H)}
 
     hbm, peak_kind = peaks()
-    # Dominant kernel: the segment walk (TswWalkKernel), timed per launch with
+    # Dominant kernel: the segment walk (TswWalkPairKernel), timed per launch with
     # CUDA events on its stream inside the library.  Algorithmic bytes are
     # those of the path itself: 3 B of RGB8 sample in and 1 B of index out per
     # pixel (4 B/px).  A launch walks `pos_per_launch` positions, so per launch
@@ -422,7 +423,7 @@ def run_ours(a, rank: int, world: int):
     frame_gbs = px * ALG_BYTES_PER_PX / (ms_step / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": TSW_TRAFFIC_PER_LAUNCH, "peak_kind": peak_kind,
-                "kernel": "TswWalkKernel", "walk_ms_per_launch": walk_ms,
+                "kernel": "TswWalkPairKernel", "walk_ms_per_launch": walk_ms,
                 "positions_per_launch": pos_per_launch,
                 "algorithmic_bytes_per_px": ALG_BYTES_PER_PX,
                 "per_frame": {"algorithmic_bytes": px * ALG_BYTES_PER_PX, "ms": ms_step,
@@ -431,11 +432,12 @@ def run_ours(a, rank: int, world: int):
                     "scratch_bytes_per_walked_position": 10,
                     "parts": "packed sample 4, uniform-key byte 1, first-touch word 4, index byte 1",
                     "ncu_dram_bytes_per_launch": TSW_TRAFFIC_PER_LAUNCH,
-                    "source": "profiles/tsw_walk_4k_rgb8_256c.md"},
+                    "source": "profiles/tsw_walk_pair_4k_rgb8_256c.md"},
                 "measured_on": "one extra step after the timed ones, host-checked pass loop, "
                                "CUDA events around each walk launch on its stream",
-                "note": "each segment is a dependent chain walked by one thread: the kernel "
-                        "is bound by the per-step chain latency, not HBM (see chain)"}
+                "note": "each segment is a dependent chain walked by a chain warp's lane, its "
+                        "running sums kept by a paired warp: the kernel is bound by the per-step "
+                        "chain latency, not HBM (see chain)"}
     clock = clk.summary()["sm_mhz"]
     lat = sb.probe_latency(dev)
     path_cycles = chain_path_cycles(lat)
