@@ -870,8 +870,74 @@ __global__ void TswVerifyKeys(TswLaunch L) {
   }
 }
 
-// The queue and own checks, one warp per walked segment.
+// The queue and own checks, one thread per walked segment (a window's
+// segments fit one wave, and a segment's own list is short).
 __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
+  int sid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L.window > 0) sid += front_of(L, 0, L.images[0].nsegs);  // the grid covers the window
+  if (sid >= total_segs) return;
+  // Owner image of this global segment id.
+  int lo = 0, hi = L.n_images - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L.images[mid].first_seg <= sid) lo = mid; else hi = mid - 1;
+  }
+  const TswImage& im = L.images[lo];
+  const int k = sid - im.first_seg;
+  if (k >= im.nsegs) return;
+  const int front = front_of(L, lo, im.nsegs);
+  if (k < front) return;  // verified earlier, not walked
+  const int wnd = window_of(L, lo);
+  if (wnd > 0 && k >= front + wnd) {
+    // Not walked this pass: the front stops at the window's end.
+    if (k == front + wnd) atomicMin(L.bad[L.pass & 1] + lo, k);
+    return;
+  }
+  // Only the image's FIRST failure matters: segments past one already found
+  // need no check.  (A relaxed read; a stale value only costs a check.)
+  if (k > *reinterpret_cast<volatile const int*>(L.bad[L.pass & 1] + lo)) return;
+  bool ok = true;
+  if (k > front) {
+    // The first walked segment started from a verified predecessor's queue;
+    // the others from their predecessor's end queue of the previous pass,
+    // which the predecessor compared with its new one (L.changed), or from a
+    // warm-up (pass 0, and segments entering a window), whose queue is
+    // compared with the predecessor's end queue itself.
+    if (L.pass == 0 || (windowed(L) && L.warmed[sid])) {
+      const double* a = L.q_start + static_cast<int64_t>(sid) * 64;
+      const double* b = L.q_end[L.pass & 1] + static_cast<int64_t>(sid - 1) * 64;
+#pragma unroll 8
+      for (int i = 0; i < 64; ++i) {
+        if (__double_as_longlong(a[i]) != __double_as_longlong(b[i])) ok = false;
+      }
+    } else if (L.changed[sid - 1]) {
+      ok = false;
+    }
+  }
+  if (ok && L.use_cache) {
+    const uint32_t* gn = im.g[L.pass & 1];
+    const uint32_t* ol = L.own_list + (static_cast<int64_t>(sid) << L.own_bits);
+    const int cnt = L.own_count[sid];
+    for (int i = 0; i < cnt && ok; ++i) {
+      const uint32_t w = ol[i];
+      const unsigned key = w & 0xFFFFFFu;
+      uint32_t g = kNone;
+      if (im.hkeys) {
+        bool present = false;
+        const int slot = map_find(im.hkeys, im.hmask, key, &present);
+        if (present) g = gn[slot];
+      } else {
+        g = gn[key];
+      }
+      if (static_cast<int>(g >> 8) < k && (g & 0xFFu) != (w >> 24)) ok = false;
+    }
+  }
+  if (!ok) atomicMin(L.bad[L.pass & 1] + lo, k);
+}
+
+// The same checks, one warp per walked segment: for long segments, whose own
+// lists run to hundreds of keys, the lanes share the list.
+__global__ void TswVerifySegmentsWarp(TswLaunch L, int total_segs) {
   int sid_lo = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (L.window > 0) sid_lo += front_of(L, 0, L.images[0].nsegs);  // the grid covers the window
@@ -1029,9 +1095,17 @@ unsigned TswWalkGrid(const TswLaunch& L) {
   if (L.window <= 0) return static_cast<unsigned>(L.n_chunks);
   return static_cast<unsigned>(std::min(L.n_chunks, (L.window + L.chunk_threads - 1) / L.chunk_threads + 1));
 }
+// Segments up to kThreadCheckLen positions are checked one thread each,
+// longer ones one warp each.
+constexpr int kThreadCheckLen = 256;
+const void* VerifyFunc(const TswLaunch& L) {
+  return L.seg_len <= kThreadCheckLen ? reinterpret_cast<const void*>(TswVerifySegments)
+                                      : reinterpret_cast<const void*>(TswVerifySegmentsWarp);
+}
 unsigned TswVerifyGrid(const TswLaunch& L, int total_segs) {
   const int segs = L.window > 0 ? std::min(total_segs, L.window + 1) : total_segs;
-  return static_cast<unsigned>((segs + 7) / 8);
+  const int per_block = L.seg_len <= kThreadCheckLen ? 256 : 8;
+  return static_cast<unsigned>((segs + per_block - 1) / per_block);
 }
 
 // The walk kernel of a launch's form and its shape: one thread per segment
@@ -1116,7 +1190,9 @@ cudaError_t LaunchTswVerify(const TswLaunch& L, int total_segs, cudaStream_t s) 
     }
   }
   if (total_segs <= 0) return cudaSuccess;
-  TswVerifySegments<<<TswVerifyGrid(L, total_segs), 256, 0, s>>>(L, total_segs);
+  void* args[] = {const_cast<TswLaunch*>(&L), &total_segs};
+  const cudaError_t e2 = cudaLaunchKernel(VerifyFunc(L), dim3(TswVerifyGrid(L, total_segs)), dim3(256), args, 0, s);
+  if (e2 != cudaSuccess) return e2;
   return cudaGetLastError();
 }
 
@@ -1178,7 +1254,7 @@ cudaError_t AddPass(cudaGraph_t g, cudaGraphNode_t* last, TswLaunch* L, int tota
   }
   if (total_segs > 0) {
     void* args2[] = {L, &total_segs};
-    e = AddKernel(g, last, reinterpret_cast<const void*>(TswVerifySegments), dim3(TswVerifyGrid(*L, total_segs)),
+    e = AddKernel(g, last, VerifyFunc(*L), dim3(TswVerifyGrid(*L, total_segs)),
                   dim3(256), 0, args2);
     if (e != cudaSuccess) return e;
   }
