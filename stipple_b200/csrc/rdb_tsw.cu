@@ -549,13 +549,8 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
           }
           if (t >= end - 16) {
             double* d = qe + 4 * (t - (end - 16));
-            const double* o = qold + 4 * (t - (end - 16));
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const double v = c < C ? e[c < C ? c : 0] : 0.0;
-              changed |= __double_as_longlong(o[c]) != __double_as_longlong(v);
-              d[c] = v;
-            }
+            for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
           }
         } else if (t >= begin - 16) {
           double* d = qs + 4 * (t - (begin - 16));
@@ -591,6 +586,18 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     if (lane == 0) atomicAdd(L.walk_count, static_cast<unsigned long long>(warp_total));
   }
   if (active && memo) L.own_count[sid] = n_own;
+  // The end queue just written against the previous pass's, once after the
+  // walk in batches of independent loads instead of a load on each of the
+  // last 16 steps.  A segment under 16 positions (an image's last) holds no
+  // full queue and has no successor: it reports a change.
+  if (active) {
+    if (end - begin >= 16) {
+#pragma unroll 16
+      for (int q = 0; q < 64; ++q) changed |= __double_as_longlong(qe[q]) != __double_as_longlong(qold[q]);
+    } else {
+      changed = true;
+    }
+  }
   if (active) {
     L.changed[sid] = changed ? 1 : 0;
     if (windowed(L)) {
