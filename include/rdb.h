@@ -248,10 +248,10 @@ typedef struct rdb_options {
   int cache_bits;       /* sequential engine: log2 shared-memory memo cache entries, 0 = auto */
   int seq_mode;         /* sequential engine: 0 = auto, 1 = one warp walks each image whole,
                            2 = speculative segmented walk on warps (exact; rdb_ssw.h),
-                           3 = the same on thread walkers, palettes without associated
-                           alpha only (exact; rdb_tsw.h).  Auto: images under 8192
-                           pixels mode 1, alpha-associated palettes mode 2, others 3.
-                           The segmented modes wait for the stream between passes. */
+                           3 = the same on thread walkers (exact; rdb_tsw.h; its forms:
+                           walk_form).  Auto: images under 8192 pixels mode 1, others 3.
+                           Mode 2 and the host-checked loop of mode 3 (loop_mode 1) wait
+                           for the stream between passes. */
   int seg_len;          /* segmented walk: positions per segment, 0 = auto */
   int warm_len;         /* segmented walk: warm-up positions before each segment, 0 = auto */
   int max_passes;       /* segmented walk: give up after this many passes (0 = no limit); the
