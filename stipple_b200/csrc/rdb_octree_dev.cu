@@ -10,7 +10,7 @@
 // the run (its colour and length), so every contribution is computed in
 // parallel; the sums are floating-point and order-dependent, so each node's
 // contributions are then added in the reference's order -- row-major run order
-// -- by one thread per node, starting from the node's value after the first
+// -- by one warp per node, starting from the node's value after the first
 // loop:
 //   1. runs: a pixel starts a run when it differs from its left neighbour (or
 //      starts its row); a scan numbers the runs in row-major order;
@@ -18,8 +18,8 @@
 //      per run: its leaf key;
 //   3. a stable radix sort by key groups each node's contributions in run
 //      order (stable sorts keep the input order within a key);
-//   4. one thread per node adds them in that order; one thread per leaf adds
-//      the run totals in order.
+//   4. one warp per node adds them in that order (its lanes load 32 at a
+//      time); one warp per leaf adds the run totals in order.
 // Integer counts are exact in any order.  The root's error, which the
 // reference accumulates across every visit, is summed in another order: its
 // exact bits decide nothing once it exceeds every other node's error (see
