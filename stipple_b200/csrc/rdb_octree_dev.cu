@@ -135,28 +135,36 @@ __device__ __forceinline__ int find_key(const uint64_t* keys, int n, uint64_t k)
 
 // One warp per node: its error from the first loop's value, then every
 // contribution in run order; and the sum of its running values (what the root
-// gains from it).  The 32 lanes load 32 contributions at a time and the warp
-// adds them one by one in order (every lane keeps the same two chains), so
-// the sums are the sequential ones bit for bit while the loads run in
-// parallel -- a node can hold millions of contributions.
+// gains from it).  The 32 lanes load 32 contributions at a time into shared
+// memory (the next 32 in flight meanwhile) and lane 0 adds them one by one in
+// order, so the sums are the sequential ones bit for bit while the loads run
+// in parallel -- a node can hold millions of contributions.
 __global__ void NodeSums(const OctreeRowsLaunch L, const uint64_t* ukeys, const int* offset,
                          const int* count, const int* nseg, const double* vals, double* qerr,
                          double* gain) {
+  __shared__ double buf[8][32];
   const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
   if (s >= *nseg) return;
   const int at = find_key(L.init_keys, L.init_n, ukeys[s]);
   double acc = at >= 0 ? L.init_qerr[at] : 0.0;
   double g = 0.0;
   const double* v = vals + offset[s];
   const int n = count[s];
+  double next = lane < n ? v[lane] : 0.0;
   for (int base = 0; base < n; base += 32) {
-    const double mine = base + lane < n ? v[base + lane] : 0.0;
-    const int m = min(32, n - base);
-    for (int j = 0; j < m; ++j) {
-      acc = __dadd_rn(acc, __shfl_sync(0xffffffffu, mine, j));
-      g = __dadd_rn(g, acc);
+    buf[w][lane] = next;
+    __syncwarp();
+    next = base + 32 + lane < n ? v[base + 32 + lane] : 0.0;
+    if (lane == 0) {
+      const int m = min(32, n - base);
+      for (int j = 0; j < m; ++j) {
+        acc = __dadd_rn(acc, buf[w][j]);
+        g = __dadd_rn(g, acc);
+      }
     }
+    __syncwarp();
   }
   if (lane == 0) {
     qerr[s] = acc;
@@ -165,51 +173,53 @@ __global__ void NodeSums(const OctreeRowsLaunch L, const uint64_t* ukeys, const 
 }
 
 // One warp per leaf: count and totals, runs in order (rd_octree.cpp:355-359).
-// Each lane forms one run's four weighted terms; the warp adds them in run
-// order, 32 runs at a time.
+// Each lane forms one run's four weighted terms into shared memory; lanes 0..3
+// then add channel 0..3 in run order, 32 runs at a time.
 __global__ void LeafSums(const OctreeRowsLaunch L, const uint64_t* ukeys, const int* offset,
                          const int* count, const int* nseg, const int* runs_sorted,
                          const int* first, int runs, uint64_t* number, double* totals) {
+  __shared__ double buf[8][32][4];
   const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
   if (s >= *nseg) return;
   const int at = find_key(L.init_keys, L.init_n, ukeys[s]);
   unsigned long long num = at >= 0 ? L.init_count[at] : 0;
-  double t[4] = {0.0, 0.0, 0.0, 0.0};
-  if (at >= 0) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) t[c] = L.init_total[4 * at + c];
-  }
+  double t = 0.0;  // lane c < 4: channel c's total
+  if (at >= 0 && lane < 4) t = L.init_total[4 * at + lane];
   const int n = count[s];
+  const int* rs = runs_sorted + offset[s];
+  int r_next = lane < n ? rs[lane] : 0;
   for (int base = 0; base < n; base += 32) {
-    double term[4] = {0.0, 0.0, 0.0, 0.0};
+    const int r = r_next;
+    r_next = base + 32 + lane < n ? rs[base + 32 + lane] : 0;
     unsigned long long run_len = 0;
+    double term[4] = {0.0, 0.0, 0.0, 0.0};
     if (base + lane < n) {
-      const int r = runs_sorted[offset[s] + base + lane];
       const int64_t p = first[r];
       const int64_t next = r + 1 < runs ? first[r + 1] : L.pixels_n;
       double px[4];
       associate(L.assoc != 0, pixel_at(L, p), px);
-      const double w = __dmul_rn(static_cast<double>(next - p), kQuantumScale);
+      const double wgt = __dmul_rn(static_cast<double>(next - p), kQuantumScale);
       run_len = static_cast<unsigned long long>(next - p);
-      term[0] = __dmul_rn(w, static_cast<double>(clamp_pixel(px[0])));
-      term[1] = __dmul_rn(w, static_cast<double>(clamp_pixel(px[1])));
-      term[2] = __dmul_rn(w, static_cast<double>(clamp_pixel(px[2])));
-      term[3] = __dmul_rn(w, static_cast<double>(clamp_pixel(L.assoc ? px[3] : kOpaqueAlpha)));
+      term[0] = __dmul_rn(wgt, static_cast<double>(clamp_pixel(px[0])));
+      term[1] = __dmul_rn(wgt, static_cast<double>(clamp_pixel(px[1])));
+      term[2] = __dmul_rn(wgt, static_cast<double>(clamp_pixel(px[2])));
+      term[3] = __dmul_rn(wgt, static_cast<double>(clamp_pixel(L.assoc ? px[3] : kOpaqueAlpha)));
     }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) buf[w][lane][c] = term[c];
     // A run lies within one row, so 32 of them sum below 2^32.
     num += __reduce_add_sync(0xffffffffu, static_cast<unsigned>(run_len));
-    const int m = min(32, n - base);
-    for (int j = 0; j < m; ++j) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) t[c] = __dadd_rn(t[c], __shfl_sync(0xffffffffu, term[c], j));
+    __syncwarp();
+    if (lane < 4) {
+      const int m = min(32, n - base);
+      for (int j = 0; j < m; ++j) t = __dadd_rn(t, buf[w][j][lane]);
     }
+    __syncwarp();
   }
-  if (lane == 0) {
-    number[s] = num;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) totals[4 * s + c] = t[c];
-  }
+  if (lane == 0) number[s] = num;
+  if (lane < 4) totals[4 * s + lane] = t;
 }
 
 unsigned Blocks(int64_t n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
