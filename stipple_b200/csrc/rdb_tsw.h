@@ -1,5 +1,6 @@
 // rdb_tsw.h -- the speculative segmented walk on thread walkers: one thread
-// per segment.
+// per segment, or (the paired form) per 32 segments a chain warp that walks
+// each step's dependent chain and a sum warp that keeps their running sums.
 //
 // The exactness argument is the one of rdb_ssw.h (segments replayed from
 // guessed states, checked against their predecessors, a verified prefix that
@@ -108,9 +109,10 @@ struct TswLaunch {
   // [front, front + window) of the image, so a whole wave of resident threads
   // works at the front; the grids of the walk and of the segment checks cover
   // the window only (chunk / segment ids counted from the front's chunk).  A
-  // segment whose predecessor the previous pass did not walk starts from a
-  // cache-free warm-up, as in pass 0 (walked[pass & 1] marks the walked ones,
-  // warmed[] the ones that started from a warm-up this pass).
+  // segment whose predecessor the previous pass did not walk starts from the
+  // empty queue, without warm-up positions, and its start queue is checked
+  // like pass 0's (walked[pass & 1] marks the walked ones, warmed[] the ones
+  // that started cache-free this pass).
   int window;
   // Per-image windows (launches of several images; null = none): image i
   // walks segments [front, front + win[i]) each pass.  TswWindows sets them
