@@ -273,10 +273,11 @@ typedef struct rdb_options {
                            truncated inverse filter (jacobi_taps, jacobi_fp64), as the
                            reference's approx engine */
   int seg_window;       /* segmented thread walk: segments walked per pass beyond the verified
-                           front.  One image: 0 = automatic, as many as the device holds
-                           resident at once.  Several: > 0 shares that many among the images
-                           after every pass, in proportion to the segments each has left (at
-                           least 256 each); 0 = none.  -1 = every unverified segment each pass. */
+                           front (-1 = every unverified segment each pass).  One image: that
+                           many (0 = as many as the device holds resident at once).  Several:
+                           that many in total (0 = twice the resident segments), shared among
+                           the images after every pass in proportion to the segments each has
+                           left, at least 256 each. */
   int walk_form;        /* segmented thread walk: 1 = paired warps: per 32 segments a chain warp
                            runs each step's dependent chain and a sum warp keeps the running
                            sums of the pending pixels, handing each over through shared memory

@@ -1644,21 +1644,24 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   // pass costs seg_len steps, and the front advances about as far per pass in
   // positions, so shorter segments cost fewer steps in total, and no pass
   // walks segments far past a front only to walk them again.
-  // Windows by default for one image; for several only when asked for
-  // (seg_window > 0): the 512-image batch measured 292 ms without, 269-533 ms
-  // with windows depending on the segment length.
-  const bool windowed = o.seg_window > 0 || (o.seg_window == 0 && n == 1);
+  // Windows by default: one image the resident segments; several share
+  // twice that (the 512-image batch: 290 ms without windows; 221 ms with a
+  // shared window of twice the resident segments at 192-256 positions, 225 at
+  // once them).
+  const bool windowed = o.seg_window >= 0;
   if (seg_len <= 0) {
     const int rule = static_cast<int>(std::min<int64_t>(16384, (all_px + resident - 1) / resident));
     int bucket = 0;
     while ((int64_t{1} << (bucket + 1)) <= all_px) ++bucket;
     std::lock_guard<std::mutex> lk(SegTuneLock());
     tune = &SegTuneTable()[std::make_tuple(device_, bucket,
-                                           (assoc ? 1 : 0) + (windowed ? 2 : 0) + (paired ? 4 : 0))];
+                                           (assoc ? 1 : 0) + (windowed ? 2 : 0) + (paired ? 4 : 0) +
+                                               (n > 1 ? 8 : 0))];
     if (tune->cand.empty()) {
       const std::initializer_list<int> all = {rule, rule / 2, rule / 4, rule * 2};
       const std::initializer_list<int> win = {96, 64, 48, 128};
-      for (int c : windowed ? win : all) {
+      const std::initializer_list<int> win_batch = {256, 192, 384, 128};
+      for (int c : windowed ? (n > 1 ? win_batch : win) : all) {
         c = std::min(16384, (std::max(c, windowed ? 32 : 64) + 15) & ~15);
         if (std::find(tune->cand.begin(), tune->cand.end(), c) == tune->cand.end()) tune->cand.push_back(c);
       }
@@ -1811,7 +1814,8 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.window = 0;
   L.win = nullptr;
   if (windowed) {
-    const int w = o.seg_window > 0 ? o.seg_window : static_cast<int>(std::min<int64_t>(resident, total));
+    const int w = o.seg_window > 0 ? o.seg_window
+                                   : static_cast<int>(std::min<int64_t>((n > 1 ? 2 : 1) * resident, total));
     if (w < total) {
       if (n == 1) {
         L.window = std::max(1, w);

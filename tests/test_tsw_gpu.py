@@ -248,7 +248,8 @@ def test_thread_segmented_batch_windows(ctx, oracle, window, form):
     """Several images in one call, each walking its own window of segments
     past its front, the windows re-shared after every pass by the segments
     each image has left (window: the total shared out, at least 256 each;
-    0 and -1: no windows for several images); both pass loops."""
+    0: twice the device's resident segments; -1: no windows); both pass
+    loops."""
     sizes = [(300, 170), (64, 140), (511, 97), (128, 128), (97, 61)]
     imgs, pids, want = [], [], []
     for k, (w, h) in enumerate(sizes):
