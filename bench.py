@@ -36,6 +36,9 @@ sys.path.insert(0, ROOT)
 HEADLINE = dict(width=3840, height=2160, colors=256, seed=1)
 # Algorithmic bytes per pixel of the path: 3 B RGB8 sample in, 1 B index out.
 ALG_BYTES_PER_PX = 4
+# Untimed calls before a timed region: the segment-length tuner's untimed
+# first call and one timed call per candidate (five) settle in them.
+WARM_CALLS = 7
 # DRAM bytes (read + write) of one walk launch of the 4K walk in its default
 # form (TswWalkPairKernel: 96-position segments, a window of the resident
 # ones), from one ncu capture (profiles/tsw_walk_pair_4k_rgb8_256c.md).
@@ -360,7 +363,7 @@ def run_ours(a, rank: int, world: int):
 
     # At least five warm-up steps: the segment-length autotuner tries four
     # lengths on its first calls for a workload.
-    for _ in range(max(5, a.warmup)):
+    for _ in range(max(WARM_CALLS, a.warmup)):
         step_dev()
     ctx.synchronize(s)
     if world > 1:
@@ -400,7 +403,7 @@ def run_ours(a, rank: int, world: int):
     pinned_in = torch.from_numpy(img).pin_memory()
     pinned_out = torch.empty((H, W), dtype=torch.uint8).pin_memory()
     e2e_t = []
-    w_e2e = max(5, a.warmup)
+    w_e2e = max(WARM_CALLS, a.warmup)
     for k in range(w_e2e + a.steps):
         t0 = time.perf_counter()
         ctx.dither_host_into("seq", pinned_in.numpy(), pid, pinned_out.numpy())
@@ -476,7 +479,7 @@ def run_ours(a, rank: int, world: int):
                                   "256-colour octree palette, bit-exact",
                       "width": W, "height": H, "colors": C, "palette_colors": tree.count,
                       "l2": "flushed between timed steps (256 MB write)",
-                      "warmup_steps_run": max(5, a.warmup),
+                      "warmup_steps_run": max(WARM_CALLS, a.warmup),
                       "parallelism": f"replicas x{world}"},
            "e2e": e2e, "roofline": roofline, "chain": chain, "clocks": clk.summary(),
            "config2_1080p": fhd, "e2e_rgbaf_inplace": rgbaf,
@@ -521,7 +524,7 @@ def bench_frame_size(ctx, s, a, W, H):
                indices=d_idx.data_ptr())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    for _ in range(max(5, a.warmup)):
+    for _ in range(max(WARM_CALLS, a.warmup)):
         ctx.dither("seq", [job], stream=s)
     ctx.synchronize(s)
     times = []
@@ -703,7 +706,7 @@ def bench_batched(ctx, s, a):
     e1.record(torch.cuda.current_stream())
     ctx.synchronize(s)
     ms_cold = e0.elapsed_time(e1)
-    for _ in range(max(5, a.warmup)):  # the segment-length autotuner explores here
+    for _ in range(max(WARM_CALLS, a.warmup)):  # the segment-length autotuner explores here
         ctx.dither("seq", jobs, stream=s)
     ctx.synchronize(s)
     e0 = torch.cuda.Event(enable_timing=True)

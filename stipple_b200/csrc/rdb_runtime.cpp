@@ -1659,7 +1659,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
                                                (n > 1 ? 8 : 0))];
     if (tune->cand.empty()) {
       const std::initializer_list<int> all = {rule, rule / 2, rule / 4, rule * 2};
-      const std::initializer_list<int> win = {96, 64, 48, 128};
+      const std::initializer_list<int> win = {96, 64, 48, 128, 32};
       const std::initializer_list<int> win_batch = {256, 192, 384, 128};
       for (int c : windowed ? (n > 1 ? win_batch : win) : all) {
         c = std::min(16384, (std::max(c, windowed ? 32 : 64) + 15) & ~15);
