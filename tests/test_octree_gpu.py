@@ -83,3 +83,16 @@ def test_flat_runs(ctx, oracle):
     """Long runs of equal pixels (weights above 1) and rows that repeat."""
     img = np.repeat(np.repeat(synth.gradient_rgb8(40, 30, 2), 8, axis=1), 4, axis=0)
     _check(ctx, oracle, img, 32, False, False)
+
+
+def test_profiled_build_reports_its_parts(ctx, oracle):
+    """With profiling on, the build's wall time by part: the host's first loop,
+    the device classification and the host reduction each took some."""
+    img = synth.gradient_rgb8(640, 480, 17)
+    ctx.profile(True)
+    try:
+        _check(ctx, oracle, img, 64, False, False)
+        parts = list(ctx.stats()["octree_ms"])
+    finally:
+        ctx.profile(False)
+    assert parts[0] > 0 and parts[1] > 0 and parts[3] > 0, parts

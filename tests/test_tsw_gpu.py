@@ -267,3 +267,29 @@ def test_thread_segmented_batch_windows(ctx, oracle, window, form):
     finally:
         for p in pids:
             ctx.release_palette(p)
+
+
+def test_profiled_walk_reports_its_work(ctx, oracle):
+    """With profiling on, the walk's statistics: one walk launch per pass,
+    every image position walked at least once (counted on the device), the
+    segment length asked for."""
+    img = synth.gradient_rgb8(400, 300, 14)
+    t = sb.Octree(img, 64, False)
+    pid = ctx.palette_from_octree(t)
+    try:
+        want, _, _ = oracle.walk_seq(synth.to_q16(img), 64, False, t.grayscale)
+        for form in (1, 2):
+            ctx.profile(True)
+            try:
+                got = ctx.dither_host("seq", img, pid, seq_mode=3, seg_len=48, warm_len=16,
+                                      seg_window=300, walk_form=form, loop_mode=1)
+                k = ctx.stats()
+            finally:
+                ctx.profile(False)
+            assert np.array_equal(got, want), form
+            assert k["passes"] == ctx.last_passes == k["walk_launches"]
+            assert k["seg_len"] == 48
+            assert k["walk_positions"] >= 400 * 300
+            assert k["walk_ms"] > 0
+    finally:
+        ctx.release_palette(pid)
