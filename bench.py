@@ -37,7 +37,8 @@ HEADLINE = dict(width=3840, height=2160, colors=256, seed=1)
 # Algorithmic bytes per pixel of the path: 3 B RGB8 sample in, 1 B index out.
 ALG_BYTES_PER_PX = 4
 # Untimed calls before a timed region: the segment-length tuner's untimed
-# first call and one timed call per candidate (five) settle in them.
+# first call and one timed call per candidate (four) settle in them, with
+# room to spare.
 WARM_CALLS = 7
 # DRAM bytes (read + write) of one walk launch of the 4K walk in its default
 # form (TswWalkPairKernel: 96-position segments, a window of the resident

@@ -1659,7 +1659,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
                                                (n > 1 ? 8 : 0))];
     if (tune->cand.empty()) {
       const std::initializer_list<int> all = {rule, rule / 2, rule / 4, rule * 2};
-      const std::initializer_list<int> win = {96, 64, 48, 128, 32};
+      const std::initializer_list<int> win = {96, 64, 48, 128};
       const std::initializer_list<int> win_batch = {256, 192, 384, 128};
       for (int c : windowed ? (n > 1 ? win_batch : win) : all) {
         c = std::min(16384, (std::max(c, windowed ? 32 : 64) + 15) & ~15);
@@ -1846,7 +1846,7 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
         const std::size_t cap = hcap[static_cast<std::size_t>(i)];
         cudaMemsetAsync(im.g[0], 0xFF, 3 * cap * sizeof(uint32_t), s);
         cudaMemsetAsync(im.hkeys, 0, cap * sizeof(uint32_t), s);
-        cudaMemsetAsync(im.hcount, 0, sizeof(int), s);
+        cudaMemsetAsync(im.hcount, 0, 3 * sizeof(int), s);  // count, classified, to classify
       } else {
         cudaMemsetAsync(im.g[1], 0xFF, kKeys * sizeof(uint32_t), s);
       }

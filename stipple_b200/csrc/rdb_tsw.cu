@@ -828,7 +828,12 @@ __global__ void TswPrepare(TswLaunch L) {
   if (m >= L.n_images) return;
   const TswImage& im = L.images[m];
   const int front = front_of(L, m, im.nsegs);
-  if (blockIdx.x == 0 && threadIdx.x == 0) L.bad[L.pass & 1][m] = 0x7F7F7F7F;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    L.bad[L.pass & 1][m] = 0x7F7F7F7F;
+    // Hashed maps: the slot list entries the last classification covered
+    // (hcount[1] .. hcount[2] of TswUniformFill) are done.
+    if (im.hkeys) im.hcount[1] = im.hcount[2];
+  }
   const uint32_t* gp = im.g[(L.pass & 1) ^ 1];
   uint32_t* gn = im.g[L.pass & 1];
   const int stride = gridDim.x * blockDim.x;
@@ -844,17 +849,23 @@ __global__ void TswPrepare(TswLaunch L) {
 // Classifies the keys of alpha-associated palettes that this pass's walk met
 // for the first time (every key it booked is in the image's hashed map):
 // rdb_uniform_alpha.cuh.  Later passes then answer the uniform ones without
-// the memo.  Images sharing a palette write the same values.
+// the memo.  Images sharing a palette write the same values.  Slots are
+// listed in insertion order and never removed, so only the list entries added
+// since the last classification need it: hcount[1] is where the last one
+// stopped, hcount[2] records where this one stops (the next pass's prepare
+// kernel moves it into hcount[1]).
 __global__ void TswUniformFill(TswLaunch L) {
   const int m = blockIdx.y;
   if (m >= L.n_images) return;
   const TswImage& im = L.images[m];
   if (!im.hkeys || !im.uni) return;
   uint8_t* table = const_cast<uint8_t*>(im.uni);
-  const int n = *im.hcount;
+  const int n = im.hcount[0];
+  const int done = im.hcount[1];
+  if (blockIdx.x == 0 && threadIdx.x == 0) im.hcount[2] = n;
   tw::Plan P;
   P.bind(im.plan);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = done + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned key = im.hkeys[im.hlist[i]] - 1u;
     if (table[key] == kUniformUnknown) table[key] = uniform_alpha_key(P, key);
   }

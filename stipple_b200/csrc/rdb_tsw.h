@@ -61,7 +61,7 @@ struct TswImage {
   // hlist[0 .. *hcount).
   uint32_t* hkeys;
   uint32_t* hlist;
-  int* hcount;
+  int* hcount;               // [0] listed slots, [1] .. [2]: uniform-key classification progress
   uint32_t hmask;
   int pad2;
 };
