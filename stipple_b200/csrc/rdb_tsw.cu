@@ -137,13 +137,8 @@ __device__ __forceinline__ void RotateTail(const double (&sw)[16], double (&R)[1
   for (int c = 0; c < C; ++c) R[U][c] = p[c];
 }
 
-// The rotations at a compile-time slot (the unrolled loop) or at a run-time
-// one (a switch over the 16 slots).
-template <int C, int U>
-__device__ __forceinline__ void RotateHeadAt(Step<U>, const double (&sw)[16], const double (&R)[16][C],
-                                             const double (&e)[C], double (&v)[C]) {
-  RotateHead<U, C>(sw, R, e, v);
-}
+// The rotations at a compile-time slot (the sum warp's unrolled loop) or at
+// a run-time one (a switch over the 16 slots).
 template <int C, int U>
 __device__ __forceinline__ void RotateTailAt(Step<U>, const double (&sw)[16], double (&R)[16][C],
                                              const double (&e)[C], const double (&p)[C]) {
