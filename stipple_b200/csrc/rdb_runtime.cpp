@@ -1814,8 +1814,14 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
   L.window = 0;
   L.win = nullptr;
   if (windowed) {
+    // One image: the walk's grid covers the window's chunks plus one, since
+    // the front need not sit on a chunk boundary; a window of the resident
+    // segments less one chunk keeps that grid within one wave of resident
+    // CTAs (with the full resident count, the extra CTA walked a second wave
+    // of seg_len steps on its own after the first).
+    const int64_t auto_w = n > 1 ? 2 * resident : std::max<int64_t>(1, resident - kChunk);
     const int w = o.seg_window > 0 ? o.seg_window
-                                   : static_cast<int>(std::min<int64_t>((n > 1 ? 2 : 1) * resident, total));
+                                   : static_cast<int>(std::min<int64_t>(auto_w, total));
     if (w < total) {
       if (n == 1) {
         L.window = std::max(1, w);
@@ -1826,6 +1832,9 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       }
     }
   }
+  // One image: its segments are dealt to the CTAs interleaved (rdb_tsw.h),
+  // with a window or without.
+  L.spread = n == 1 ? 1 : 0;
   if (L.window > 0 || L.win) cudaMemsetAsync(L.walked[0], 0, 2 * static_cast<std::size_t>(total), s);
   L.walk_count = nullptr;
   if (profiling_) {

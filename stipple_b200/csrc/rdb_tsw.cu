@@ -605,19 +605,21 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
 template <bool kFloat, bool kAssoc>
 __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
+  const bool spread = L.spread != 0;
   int chunk = blockIdx.x;
-  if (L.window > 0) {
+  if (L.window > 0 && !spread) {
     // One image: chunks are its segments 128 at a time; the grid covers the
     // window, counted from the front's chunk.
     chunk += front_of(L, 0, L.images[0].nsegs) / L.chunk_threads;
     if (chunk >= L.n_chunks) return;
   }
-  const TswChunk ch = L.chunks[chunk];
+  const TswChunk ch = L.chunks[spread ? 0 : chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
   const int wnd = window_of(L, ch.image);
   const int stop = wnd > 0 ? min(front + wnd, im.nsegs) : im.nsegs;
-  if (ch.k0 + ch.count <= front || ch.k0 >= stop) return;  // nothing to walk (uniform per CTA)
+  // Nothing to walk (uniform per CTA).
+  if (!spread && (ch.k0 + ch.count <= front || ch.k0 >= stop)) return;
   {
     const int4* src = reinterpret_cast<const int4*>(im.plan);
     int4* dst = reinterpret_cast<int4*>(smem);
@@ -639,17 +641,27 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  // Warps whose segments are all verified, past the window or past the image
-  // leave together.
-  const int warp_k0 = ch.k0 + static_cast<int>(threadIdx.x & ~31u);
-  const int warp_end = min(ch.k0 + ch.count, warp_k0 + 32);
-  if (warp_end <= front || warp_k0 >= ch.k0 + ch.count || warp_k0 >= stop) return;
-  const int k = ch.k0 + static_cast<int>(threadIdx.x);
-  const bool active = static_cast<int>(threadIdx.x) < ch.count && k >= front && k < stop;
+  int k, kk;
+  bool active;
+  if (spread) {
+    k = front / L.chunk_threads * L.chunk_threads + static_cast<int>(threadIdx.x) * static_cast<int>(gridDim.x) +
+        static_cast<int>(blockIdx.x);
+    active = k >= front && k < stop;
+    if (__ballot_sync(0xffffffffu, active) == 0u) return;  // the warp leaves together
+    kk = active ? k : front;
+  } else {
+    // Warps whose segments are all verified, past the window or past the
+    // image leave together.
+    const int warp_k0 = ch.k0 + static_cast<int>(threadIdx.x & ~31u);
+    const int warp_end = min(ch.k0 + ch.count, warp_k0 + 32);
+    if (warp_end <= front || warp_k0 >= ch.k0 + ch.count || warp_k0 >= stop) return;
+    k = ch.k0 + static_cast<int>(threadIdx.x);
+    active = static_cast<int>(threadIdx.x) < ch.count && k >= front && k < stop;
+    kk = active ? k : warp_end - 1;
+  }
   tw::Plan P;
   P.bind(smem);
-  WalkSegment<kFloat, kAssoc, false>(L, im, P, errp, active ? k : warp_end - 1, front, active, lane,
-                                     nullptr);
+  WalkSegment<kFloat, kAssoc, false>(L, im, P, errp, kk, front, active, lane, nullptr);
 }
 
 // The sum warp of a pair: the 16-slot ring of running sums for one segment
@@ -757,17 +769,19 @@ __device__ __forceinline__ void WalkSums(const TswLaunch& L, const TswImage& im,
 template <bool kFloat, bool kAssoc>
 __global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKernel(TswLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
+  const bool spread = L.spread != 0;
   int chunk = blockIdx.x;
-  if (L.window > 0) {
+  if (L.window > 0 && !spread) {
     chunk += front_of(L, 0, L.images[0].nsegs) / L.chunk_threads;
     if (chunk >= L.n_chunks) return;
   }
-  const TswChunk ch = L.chunks[chunk];
+  const TswChunk ch = L.chunks[spread ? 0 : chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
   const int wnd = window_of(L, ch.image);
   const int stop = wnd > 0 ? min(front + wnd, im.nsegs) : im.nsegs;
-  if (ch.k0 + ch.count <= front || ch.k0 >= stop) return;  // nothing to walk (uniform per CTA)
+  // Nothing to walk (uniform per CTA).
+  if (!spread && (ch.k0 + ch.count <= front || ch.k0 >= stop)) return;
   constexpr int C = kAssoc ? 4 : 3;
   double* errp = reinterpret_cast<double*>(smem + L.plan_smem_max);
   // After the plan and the residual-side colours, 16-byte aligned (as the
@@ -800,12 +814,22 @@ __global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKe
   const int warp = threadIdx.x >> 5;
   const int pair = warp % kPairsPerCta;
   // Both warps of a pair see the same 32 segments and leave together.
-  const int warp_k0 = ch.k0 + 32 * pair;
-  const int warp_end = min(ch.k0 + ch.count, warp_k0 + 32);
-  if (warp_end <= front || warp_k0 >= ch.k0 + ch.count || warp_k0 >= stop) return;
-  const int k = warp_k0 + lane;
-  const bool active = k < warp_end && k >= front && k < stop;
-  const int kk = active ? k : warp_end - 1;
+  int kk;
+  bool active;
+  if (spread) {
+    const int k = front / L.chunk_threads * L.chunk_threads +
+                  (32 * pair + lane) * static_cast<int>(gridDim.x) + static_cast<int>(blockIdx.x);
+    active = k >= front && k < stop;
+    if (__ballot_sync(0xffffffffu, active) == 0u) return;
+    kk = active ? k : front;
+  } else {
+    const int warp_k0 = ch.k0 + 32 * pair;
+    const int warp_end = min(ch.k0 + ch.count, warp_k0 + 32);
+    if (warp_end <= front || warp_k0 >= ch.k0 + ch.count || warp_k0 >= stop) return;
+    const int k = warp_k0 + lane;
+    active = k < warp_end && k >= front && k < stop;
+    kk = active ? k : warp_end - 1;
+  }
   if (warp < kPairsPerCta) {
     tw::Plan P;
     P.bind(smem);

@@ -114,6 +114,14 @@ struct TswLaunch {
   // like pass 0's (walked[pass & 1] marks the walked ones, warmed[] the ones
   // that started cache-free this pass).
   int window;
+  // One image (with a window or without): the walk's grid of G CTAs takes
+  // the segments from the front's chunk start on interleaved (CTA c, slot s
+  // of its 128 walks segment base + s * G + c) instead of 128 consecutive
+  // ones per CTA, so the segments just past the front -- where new memo
+  // keys, and with them searches, are densest -- spread over every CTA and
+  // warp rather than holding up the launch in a few.  Same segments, same
+  // results.
+  int spread;
   // Per-image windows (launches of several images; null = none): image i
   // walks segments [front, front + win[i]) each pass.  TswWindows sets them
   // after every pass from the segments each image has left: resident_segs
