@@ -1832,9 +1832,9 @@ int Context::SeqThreadSegmented(const rdb_job* jobs, int n, const rdb_options& o
       }
     }
   }
-  // One image: its segments are dealt to the CTAs interleaved (rdb_tsw.h),
-  // with a window or without.
-  L.spread = n == 1 ? 1 : 0;
+  // Segments dealt to the CTAs interleaved (rdb_tsw.h): one image with a
+  // window or without, several with per-image windows.
+  L.spread = (n == 1 || L.win) ? 1 : 0;
   if (L.window > 0 || L.win) cudaMemsetAsync(L.walked[0], 0, 2 * static_cast<std::size_t>(total), s);
   L.walk_count = nullptr;
   if (profiling_) {

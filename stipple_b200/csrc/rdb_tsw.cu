@@ -35,6 +35,29 @@ __device__ __forceinline__ int window_of(const TswLaunch& L, int image) {
 }
 __device__ __forceinline__ bool windowed(const TswLaunch& L) { return L.window > 0 || L.win != nullptr; }
 
+// The interleaved deal of TswLaunch::spread: CTA c of the g CTAs that take an
+// image's segments walks base + s * g + c in its slot s, base being the
+// front's chunk start.  One image: the whole grid.  Several (per-image
+// windows): the image's first g chunks, g covering its window (one chunk
+// more, since the front need not sit on a chunk boundary).  False when this
+// CTA takes none.
+struct Deal {
+  int base, g, c;
+};
+__device__ __forceinline__ bool deal_of(const TswLaunch& L, const TswChunk& ch, int front, int wnd,
+                                        int nsegs, Deal* d) {
+  const int ct = L.chunk_threads;
+  d->base = front / ct * ct;
+  if (L.win) {
+    d->c = ch.k0 / ct;
+    d->g = min((nsegs - d->base + ct - 1) / ct, (wnd + ct - 1) / ct + 1);
+  } else {
+    d->c = static_cast<int>(blockIdx.x);
+    d->g = static_cast<int>(gridDim.x);
+  }
+  return d->c < d->g;
+}
+
 __device__ __forceinline__ int find_image(const TswImage* imgs, int n, int64_t pos) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
@@ -613,13 +636,17 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
     chunk += front_of(L, 0, L.images[0].nsegs) / L.chunk_threads;
     if (chunk >= L.n_chunks) return;
   }
-  const TswChunk ch = L.chunks[spread ? 0 : chunk];
+  const TswChunk ch = L.chunks[spread && !L.win ? 0 : chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
   const int wnd = window_of(L, ch.image);
   const int stop = wnd > 0 ? min(front + wnd, im.nsegs) : im.nsegs;
   // Nothing to walk (uniform per CTA).
-  if (!spread && (ch.k0 + ch.count <= front || ch.k0 >= stop)) return;
+  Deal deal{0, 0, 0};
+  if (spread ? !deal_of(L, ch, front, wnd, im.nsegs, &deal)
+             : (ch.k0 + ch.count <= front || ch.k0 >= stop)) {
+    return;
+  }
   {
     const int4* src = reinterpret_cast<const int4*>(im.plan);
     int4* dst = reinterpret_cast<int4*>(smem);
@@ -644,8 +671,7 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   int k, kk;
   bool active;
   if (spread) {
-    k = front / L.chunk_threads * L.chunk_threads + static_cast<int>(threadIdx.x) * static_cast<int>(gridDim.x) +
-        static_cast<int>(blockIdx.x);
+    k = deal.base + static_cast<int>(threadIdx.x) * deal.g + deal.c;
     active = k >= front && k < stop;
     if (__ballot_sync(0xffffffffu, active) == 0u) return;  // the warp leaves together
     kk = active ? k : front;
@@ -775,13 +801,17 @@ __global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKe
     chunk += front_of(L, 0, L.images[0].nsegs) / L.chunk_threads;
     if (chunk >= L.n_chunks) return;
   }
-  const TswChunk ch = L.chunks[spread ? 0 : chunk];
+  const TswChunk ch = L.chunks[spread && !L.win ? 0 : chunk];
   const TswImage& im = L.images[ch.image];
   const int front = front_of(L, ch.image, im.nsegs);
   const int wnd = window_of(L, ch.image);
   const int stop = wnd > 0 ? min(front + wnd, im.nsegs) : im.nsegs;
   // Nothing to walk (uniform per CTA).
-  if (!spread && (ch.k0 + ch.count <= front || ch.k0 >= stop)) return;
+  Deal deal{0, 0, 0};
+  if (spread ? !deal_of(L, ch, front, wnd, im.nsegs, &deal)
+             : (ch.k0 + ch.count <= front || ch.k0 >= stop)) {
+    return;
+  }
   constexpr int C = kAssoc ? 4 : 3;
   double* errp = reinterpret_cast<double*>(smem + L.plan_smem_max);
   // After the plan and the residual-side colours, 16-byte aligned (as the
@@ -817,8 +847,7 @@ __global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKe
   int kk;
   bool active;
   if (spread) {
-    const int k = front / L.chunk_threads * L.chunk_threads +
-                  (32 * pair + lane) * static_cast<int>(gridDim.x) + static_cast<int>(blockIdx.x);
+    const int k = deal.base + (32 * pair + lane) * deal.g + deal.c;
     active = k >= front && k < stop;
     if (__ballot_sync(0xffffffffu, active) == 0u) return;
     kk = active ? k : front;

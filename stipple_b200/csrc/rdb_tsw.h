@@ -117,10 +117,11 @@ struct TswLaunch {
   // One image (with a window or without): the walk's grid of G CTAs takes
   // the segments from the front's chunk start on interleaved (CTA c, slot s
   // of its 128 walks segment base + s * G + c) instead of 128 consecutive
-  // ones per CTA, so the segments just past the front -- where new memo
-  // keys, and with them searches, are densest -- spread over every CTA and
-  // warp rather than holding up the launch in a few.  Same segments, same
-  // results.
+  // ones per CTA; with per-image windows, the image's first G chunks take
+  // its window that way, G covering the window plus one chunk.  So the
+  // segments just past the front -- where new memo keys, and with them
+  // searches, are densest -- spread over every CTA and warp rather than
+  // holding up the launch in a few.  Same segments, same results.
   int spread;
   // Per-image windows (launches of several images; null = none): image i
   // walks segments [front, front + win[i]) each pass.  TswWindows sets them
