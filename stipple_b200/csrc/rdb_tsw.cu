@@ -36,7 +36,8 @@ __device__ __forceinline__ int window_of(const TswLaunch& L, int image) {
 __device__ __forceinline__ bool windowed(const TswLaunch& L) { return L.window > 0 || L.win != nullptr; }
 
 // The interleaved deal of TswLaunch::spread: CTA c of the g CTAs that take an
-// image's segments walks base + s * g + c in its slot s, base being the
+// image's segments walks base + s * g + c in its slot s (slots numbered lane
+// by lane across the CTA's warps), base being the
 // front's chunk start.  One image: the whole grid.  Several (per-image
 // windows): the image's first g chunks, g covering its window (one chunk
 // more, since the front need not sit on a chunk boundary).  False when this
@@ -606,12 +607,16 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   if (active && memo) L.own_count[sid] = n_own;
   // The end queue just written against the previous pass's, once after the
   // walk in batches of independent loads instead of a load on each of the
-  // last 16 steps.  A segment under 16 positions (an image's last) holds no
-  // full queue and has no successor: it reports a change.
+  // last 16 steps; only the channels a walk reads (without alpha the fourth
+  // is never read, so it cannot make a successor's start wrong).  A segment
+  // under 16 positions (an image's last) holds no full queue and has no
+  // successor: it reports a change.
   if (active) {
     if (end - begin >= 16) {
 #pragma unroll 16
-      for (int q = 0; q < 64; ++q) changed |= __double_as_longlong(qe[q]) != __double_as_longlong(qold[q]);
+      for (int q = 0; q < 64; ++q) {
+        if ((q & 3) < C) changed |= __double_as_longlong(qe[q]) != __double_as_longlong(qold[q]);
+      }
     } else {
       changed = true;
     }
@@ -671,7 +676,9 @@ __global__ void __launch_bounds__(128, kAssoc ? 2 : 3) TswWalkKernel(TswLaunch L
   int k, kk;
   bool active;
   if (spread) {
-    k = deal.base + static_cast<int>(threadIdx.x) * deal.g + deal.c;
+    // Slots lane-major across the CTA's warps, so every warp gets segments
+    // from the whole window, the nearest ones included.
+    k = deal.base + (lane * 4 + static_cast<int>(threadIdx.x >> 5)) * deal.g + deal.c;
     active = k >= front && k < stop;
     if (__ballot_sync(0xffffffffu, active) == 0u) return;  // the warp leaves together
     kk = active ? k : front;
@@ -847,7 +854,9 @@ __global__ void __launch_bounds__(kPairCtaThreads, kAssoc ? 1 : 2) TswWalkPairKe
   int kk;
   bool active;
   if (spread) {
-    const int k = deal.base + (32 * pair + lane) * deal.g + deal.c;
+    // Slots lane-major across the pairs, so every pair gets segments from the
+    // whole window, the nearest ones included.
+    const int k = deal.base + (lane * kPairsPerCta + pair) * deal.g + deal.c;
     active = k >= front && k < stop;
     if (__ballot_sync(0xffffffffu, active) == 0u) return;
     kk = active ? k : front;

@@ -101,9 +101,9 @@ struct TswLaunch {
   // prefix -- and writes bad[p & 1].
   int* bad[2];
   // Per segment, written by every walk from pass 1 on: 1 when the segment's end
-  // queue differs from the one it ended with in the previous pass -- exactly
-  // when the next segment, which started from that previous queue, started
-  // from the wrong one.
+  // queue differs from the one it ended with in the previous pass, in the
+  // channels a walk reads -- exactly when the next segment, which started
+  // from that previous queue, started from the wrong one.
   uint8_t* changed;
   // Window (single-image launches; 0 = none): a pass walks only segments
   // [front, front + window) of the image, so a whole wave of resident threads
@@ -116,9 +116,10 @@ struct TswLaunch {
   int window;
   // One image (with a window or without): the walk's grid of G CTAs takes
   // the segments from the front's chunk start on interleaved (CTA c, slot s
-  // of its 128 walks segment base + s * G + c) instead of 128 consecutive
-  // ones per CTA; with per-image windows, the image's first G chunks take
-  // its window that way, G covering the window plus one chunk.  So the
+  // of its 128 walks segment base + s * G + c, the slots numbered lane by
+  // lane across its warps) instead of 128 consecutive ones per CTA; with
+  // per-image windows, the image's first G chunks take its window that way,
+  // G covering the window plus one chunk.  So the
   // segments just past the front -- where new memo keys, and with them
   // searches, are densest -- spread over every CTA and warp rather than
   // holding up the launch in a few.  Same segments, same results.
