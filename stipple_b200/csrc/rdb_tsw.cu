@@ -428,13 +428,24 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
   // One step of the walk; U = the step index mod 16 is a compile-time
   // constant, so the running sums stay in fixed registers with no
   // indexed jump per step.
+  // The paired form compares its end queue step by step: each of the last 16
+  // steps loads the previous pass's entry before waiting for its sum, so the
+  // comparison waits for nothing (the one-thread form compares once after
+  // the walk, below).
+  const bool cmp_steps = kChain && active && end - begin >= 16;
   const auto step = [&](auto u, const int i) -> bool {
+      const bool on = i < steps;
+      const int t = ws + i;
+      const bool cmp = cmp_steps && on && t >= end - 16;
+      long long qo[C];
+      if (cmp) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) qo[c] = __double_as_longlong(qold[4 * (t - (end - 16)) + c]);
+      }
       if constexpr (kChain) {
         // Pixel t's running sum from the sum warp (every lane waits).
         if (!pair_wait(&box->full_s[i & 1], (i >> 1) & 1, L.status)) return false;
       }
-      const bool on = i < steps;
-      const int t = ws + i;
       float f[4] = {0.0f, 0.0f, 0.0f, 0.0f};
       unsigned br = 0, bg = 0, bb = 0, ba = 0, key = 0, h = 0;
       int index = 0, slot = 0;
@@ -570,6 +581,10 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
             double* d = qe + 4 * (t - (end - 16));
 #pragma unroll
             for (int c = 0; c < 4; ++c) d[c] = c < C ? e[c < C ? c : 0] : 0.0;
+            if (cmp) {
+#pragma unroll
+              for (int c = 0; c < C; ++c) changed |= qo[c] != __double_as_longlong(e[c]);
+            }
           }
         } else if (t >= begin - 16) {
           double* d = qs + 4 * (t - (begin - 16));
@@ -605,13 +620,13 @@ __device__ __forceinline__ void WalkSegment(const TswLaunch& L, const TswImage& 
     if (lane == 0) atomicAdd(L.walk_count, static_cast<unsigned long long>(warp_total));
   }
   if (active && memo) L.own_count[sid] = n_own;
-  // The end queue just written against the previous pass's, once after the
-  // walk in batches of independent loads instead of a load on each of the
-  // last 16 steps; only the channels a walk reads (without alpha the fourth
+  // One thread a segment: the end queue just written against the previous
+  // pass's, once after the walk in batches of independent loads instead of a
+  // load on each of the last 16 steps; only the channels a walk reads (without alpha the fourth
   // is never read, so it cannot make a successor's start wrong).  A segment
   // under 16 positions (an image's last) holds no full queue and has no
   // successor: it reports a change.
-  if (active) {
+  if (active && !cmp_steps) {
     if (end - begin >= 16) {
 #pragma unroll 16
       for (int q = 0; q < 64; ++q) {
