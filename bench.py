@@ -43,7 +43,7 @@ WARM_CALLS = 7
 # DRAM bytes (read + write) of one walk launch of the 4K walk in its default
 # form (TswWalkPairKernel: 96-position segments, a window of the resident
 # ones), from one ncu capture (profiles/tsw_walk_pair_4k_rgb8_256c.md).
-TSW_TRAFFIC_PER_LAUNCH = 37409024 + 1372160
+TSW_TRAFFIC_PER_LAUNCH = 37494784 + 871168
 # The per-step dependent path of the thread walker, as a sum of measured
 # latencies (rdb_probe_latency on the same GPU): the head's DMUL and DADD,
 # double -> float (clamp), float -> int and the byte rule's integer ops, the
