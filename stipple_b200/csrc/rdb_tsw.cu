@@ -1008,18 +1008,30 @@ __global__ void TswVerifySegments(TswLaunch L, int total_segs) {
     const uint32_t* gn = im.g[L.pass & 1];
     const uint32_t* ol = L.own_list + (static_cast<int64_t>(sid) << L.own_bits);
     const int cnt = L.own_count[sid];
-    for (int i = 0; i < cnt && ok; ++i) {
-      const uint32_t w = ol[i];
-      const unsigned key = w & 0xFFFFFFu;
-      uint32_t g = kNone;
-      if (im.hkeys) {
+    if (im.hkeys) {
+      for (int i = 0; i < cnt && ok; ++i) {
+        const uint32_t w = ol[i];
+        uint32_t g = kNone;
         bool present = false;
-        const int slot = map_find(im.hkeys, im.hmask, key, &present);
+        const int slot = map_find(im.hkeys, im.hmask, w & 0xFFFFFFu, &present);
         if (present) g = gn[slot];
-      } else {
-        g = gn[key];
+        if (static_cast<int>(g >> 8) < k && (g & 0xFFu) != (w >> 24)) ok = false;
       }
-      if (static_cast<int>(g >> 8) < k && (g & 0xFFu) != (w >> 24)) ok = false;
+    } else {
+      // Direct maps: eight entries at a time, their list words and then their
+      // map words loaded independently, so a long list costs a few round
+      // trips instead of two dependent loads an entry.
+      for (int i0 = 0; i0 < cnt && ok; i0 += 8) {
+        uint32_t w[8], g[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) w[j] = i0 + j < cnt ? ol[i0 + j] : 0u;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) g[j] = i0 + j < cnt ? gn[w[j] & 0xFFFFFFu] : kNone;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (static_cast<int>(g[j] >> 8) < k && (g[j] & 0xFFu) != (w[j] >> 24)) ok = false;
+        }
+      }
     }
   }
   if (!ok) atomicMin(L.bad[L.pass & 1] + lo, k);
