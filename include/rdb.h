@@ -274,7 +274,8 @@ typedef struct rdb_options {
                            reference's approx engine */
   int seg_window;       /* segmented thread walk: segments walked per pass beyond the verified
                            front (-1 = every unverified segment each pass).  One image: that
-                           many (0 = as many as the device holds resident at once).  Several:
+                           many (0 = as many as the device holds resident at once, less one
+                           CTA's 128, so the pass stays one wave).  Several:
                            that many in total (0 = twice the resident segments), shared among
                            the images after every pass in proportion to the segments each has
                            left, at least 256 each. */
