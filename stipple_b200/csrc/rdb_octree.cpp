@@ -164,6 +164,11 @@ void Octree::Colormap(int32_t node) {
 void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int colors_level) {
   const Sample* row = reinterpret_cast<const Sample*>(rgba);
   const double midpoint = kQuantumRange / 2.0;
+  // The root's running error, which every visited node's error is added to
+  // in visit order: kept in a register for the row (the descent never
+  // visits the root itself, so no other read sees it meanwhile) instead of
+  // a store and reload through the node array at every level.
+  double root = nodes_[0].qerr;
   std::size_t x = 0;
   while (x < width) {
     std::size_t run = 1;
@@ -204,7 +209,7 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
       double dist = e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3;
       if (std::isnan(dist)) dist = 0.0;
       nodes_[node].qerr += weight * std::sqrt(dist);
-      nodes_[0].qerr += nodes_[node].qerr;
+      root += nodes_[node].qerr;
     }
     OctNode& leaf = nodes_[node];
     leaf.number_unique += run;
@@ -215,6 +220,7 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
                      static_cast<double>(clamp_pixel(assoc_ ? px[3] : kOpaqueAlpha));
     x += run;
   }
+  nodes_[0].qerr = root;
 }
 
 void Octree::Setup(int max_colors, bool associate_alpha, bool grayscale) {

@@ -13,7 +13,11 @@
 
 namespace rdb {
 
-struct OctNode {
+// 128 bytes on a 64-byte boundary: the error and the child table share the
+// first cache line, so a level of the classification descent (child lookup,
+// error update) touches one line; counts and totals (leaves only) the second.
+struct alignas(64) OctNode {
+  double qerr;
   int32_t child[16];
   int32_t parent;
   uint32_t id;
@@ -21,8 +25,8 @@ struct OctNode {
   uint32_t color_number;
   uint64_t number_unique;
   double total[4];
-  double qerr;
 };
+static_assert(sizeof(OctNode) == 128, "OctNode is two cache lines");
 
 struct PaletteColor {
   double r, g, b, a;
