@@ -866,14 +866,20 @@ def run_reference(a):
     img = synth.gradient_rgb8(W, H, HEADLINE["seed"])
     for _ in range(max(1, min(a.warmup, 1))):
         reference_cpu(img, C, budget_s=0.0)
-    cpu, times = reference_cpu(img, C, budget_s=0.0)
     step_times = []
-    for _ in range(a.steps):
-        c, t = reference_cpu(img, C, budget_s=0.0)
+    cpu = {}
+    for _ in range(max(1, a.steps)):
+        cpu, t = reference_cpu(img, C, budget_s=0.0)
         step_times.extend(t)
     ms = statistics.median(step_times) * 1e3
     value = W * H / ms / 1e3
-    cpu["value"] = value
+    # The baseline record describes the timed steps themselves.
+    q1, q3 = (float(v) for v in np.percentile(step_times, [25, 75]))
+    cpu.update({"value": value, "iqr_mpx_s": [W * H / q3 / 1e6, W * H / q1 / 1e6],
+                "runs": len(step_times),
+                "sample": f"{len(step_times)} sequential walks of the {W}x{H} frame ({C} colours), "
+                          "median, palette build excluded; the walk is one dependent chain, so "
+                          "one thread"})
     return {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded gradient + noise sigma 8, RGB8)",
