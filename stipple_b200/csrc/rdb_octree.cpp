@@ -160,8 +160,20 @@ void Octree::Colormap(int32_t node) {
 }
 
 // rd_octree.cpp:305-362: one row, run-length collapsed, each run descending to
-// `level_limit` and counting new nodes at `colors_level` as colours.
+// `level_limit` and counting new nodes at `colors_level` as colours.  The
+// alpha channel is a compile-time choice: without it the fourth midpoint and
+// the fourth (zero) term of the distance are not computed, which changes no
+// sum (a sum of squares plus +0.0 is itself).
 void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int colors_level) {
+  if (assoc_) {
+    ClassifyAs<true>(rgba, width, level_limit, colors_level);
+  } else {
+    ClassifyAs<false>(rgba, width, level_limit, colors_level);
+  }
+}
+
+template <bool kAssoc>
+void Octree::ClassifyAs(const float* rgba, std::size_t width, int level_limit, int colors_level) {
   const Sample* row = reinterpret_cast<const Sample*>(rgba);
   const double midpoint = kQuantumRange / 2.0;
   // The root's running error, which every visited node's error is added to
@@ -178,7 +190,7 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
       ++run;
     }
     double px[4];
-    Associate(assoc_, row[x], px);
+    Associate(kAssoc, row[x], px);
     unsigned byte[4];
     for (int c = 0; c < 4; ++c) byte[c] = scale_char(clamp_pixel(px[c]));
     double half = (kQuantumRange + 1.0) / 2.0;
@@ -190,11 +202,11 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
       half *= 0.5;
       unsigned id = ((byte[0] >> bit) & 1u) | (((byte[1] >> bit) & 1u) << 1) |
                     (((byte[2] >> bit) & 1u) << 2);
-      if (assoc_) id |= ((byte[3] >> bit) & 1u) << 3;
+      if (kAssoc) id |= ((byte[3] >> bit) & 1u) << 3;
       mid[0] += (id & 1u) ? half : -half;
       mid[1] += (id & 2u) ? half : -half;
       mid[2] += (id & 4u) ? half : -half;
-      mid[3] += (id & 8u) ? half : -half;
+      if (kAssoc) mid[3] += (id & 8u) ? half : -half;
       if (nodes_[node].child[id] < 0) {
         const int32_t made = Add(id, static_cast<uint32_t>(level), node);
         nodes_[node].child[id] = made;
@@ -205,8 +217,11 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
       const double e0 = kQuantumScale * (px[0] - mid[0]);
       const double e1 = kQuantumScale * (px[1] - mid[1]);
       const double e2 = kQuantumScale * (px[2] - mid[2]);
-      const double e3 = assoc_ ? (kQuantumScale * (px[3] - mid[3])) : 0.0;
-      double dist = e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3;
+      double dist = e0 * e0 + e1 * e1 + e2 * e2;
+      if (kAssoc) {
+        const double e3 = kQuantumScale * (px[3] - mid[3]);
+        dist = dist + e3 * e3;
+      }
       if (std::isnan(dist)) dist = 0.0;
       nodes_[node].qerr += weight * std::sqrt(dist);
       root += nodes_[node].qerr;
@@ -217,7 +232,7 @@ void Octree::Classify(const float* rgba, std::size_t width, int level_limit, int
     leaf.total[1] += weight * kQuantumScale * static_cast<double>(clamp_pixel(px[1]));
     leaf.total[2] += weight * kQuantumScale * static_cast<double>(clamp_pixel(px[2]));
     leaf.total[3] += weight * kQuantumScale *
-                     static_cast<double>(clamp_pixel(assoc_ ? px[3] : kOpaqueAlpha));
+                     static_cast<double>(clamp_pixel(kAssoc ? px[3] : kOpaqueAlpha));
     x += run;
   }
   nodes_[0].qerr = root;

@@ -99,6 +99,8 @@ class Octree {
   int32_t Add(uint32_t id, uint32_t level, int32_t parent);
   int Fan() const { return assoc_ ? 16 : 8; }
   void Classify(const float* rgba, std::size_t width, int level_limit, int colors_level);
+  template <bool kAssoc>
+  void ClassifyAs(const float* rgba, std::size_t width, int level_limit, int colors_level);
   void Merge(int32_t node);
   void PruneAtDepth(int32_t node);
   void PruneBelowDepth(int32_t node);
